@@ -1,0 +1,962 @@
+// dpg_host.cu — plan construction and the C ABI of the DPG assembly library.
+//
+// The plan reproduces, for one bucket (Camellia ElementType), what
+// BasisCache/BasisFactory/DofOrdering set up on the CPU in the reference:
+//   - tensor Gauss rules, n = degree/2 + 1 points per direction
+//     (src/Basis/CubatureFactory.cpp:25-53, degrees src/Basis/BasisCache.cpp:68-84,236-267,198-222);
+//   - reference bases (src/Basis/BasisFactory.cpp:122-420): HGRAD Cn nodal at
+//     Gauss-Lobatto points (x fastest), HDIV In = tensor Raviart-Thomas
+//     (component-major), HVOL of H1Order k = HGRAD C(k-1), VECTOR_HVOL =
+//     component-major copies; traces: HGRAD C(k) / HVOL C(k-1) on each side in
+//     the side's own parametrisation (shards side node order);
+//   - dof numbering var by var, traces side by side
+//     (src/DofOrdering/DofOrderingFactory.cpp:53-211, DofOrdering.cpp:27-60).
+// The tables are uploaded once; the kernels apply the Piola transforms per cell.
+#include "../../include/dpg_b200.h"
+#include "dpg_plan.h"
+#include "dpg_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace dpg {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+// ----------------------------------------------------------------------------
+// 1D point families
+// ----------------------------------------------------------------------------
+
+// P_n(x) and P_n'(x)
+static void legendre_pd(int n, double x, double* p, double* dp) {
+  double a = 1.0, b = x;  // P_0, P_1
+  if (n == 0) { *p = 1.0; *dp = 0.0; return; }
+  for (int m = 1; m < n; m++) {
+    double c = ((2 * m + 1) * x * b - m * a) / (m + 1);
+    a = b;
+    b = c;
+  }
+  *p = b;
+  *dp = n * (x * b - a) / (x * x - 1.0);
+}
+
+// n-point Gauss-Legendre rule, nodes ascending.
+static void gauss_rule(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.resize(n);
+  w.resize(n);
+  for (int i = 0; i < n; i++) {
+    // Tricomi initial guess, refined by Newton
+    double z = std::cos(M_PI * (n - i - 0.25) / (n + 0.5));
+    for (int it = 0; it < 60; it++) {
+      double p, dp;
+      legendre_pd(n, z, &p, &dp);
+      double step = p / dp;
+      z -= step;
+      if (std::fabs(step) <= 1e-17) break;
+    }
+    double p, dp;
+    legendre_pd(n, z, &p, &dp);
+    x[i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+// Gauss-Lobatto-Legendre nodes of degree p (p+1 nodes).
+static std::vector<double> gll_nodes(int p) {
+  std::vector<double> x(p + 1, 0.0);
+  if (p == 0) return x;
+  x[0] = -1.0;
+  x[p] = 1.0;
+  for (int i = 1; i < p; i++) {
+    double z = -std::cos(M_PI * i / p);
+    for (int it = 0; it < 60; it++) {
+      double P, dP;
+      legendre_pd(p, z, &P, &dP);
+      // Newton on (1 - z^2) P'(z): derivative = -p(p+1) P(z) by Legendre's equation
+      double f = (1.0 - z * z) * dP;
+      double df = -p * (p + 1.0) * P;
+      double step = f / df;
+      z -= step;
+      if (std::fabs(step) <= 1e-17) break;
+    }
+    x[i] = z;
+  }
+  return x;
+}
+
+struct Lagrange1D {
+  std::vector<double> x;
+  int n() const { return (int)x.size(); }
+  // values and derivatives of all polynomials at s
+  void eval(double s, double* v, double* dv) const {
+    int m = n();
+    if (m == 1) { v[0] = 1.0; dv[0] = 0.0; return; }
+    for (int j = 0; j < m; j++) {
+      double num = 1.0, den = 1.0, der = 0.0;
+      for (int k = 0; k < m; k++) {
+        if (k == j) continue;
+        den *= (x[j] - x[k]);
+        // derivative of prod_k (s - x_k): sum over the factor left out
+        double term = 1.0;
+        for (int q = 0; q < m; q++)
+          if (q != j && q != k) term *= (s - x[q]);
+        der += term;
+        num *= (s - x[k]);
+      }
+      v[j] = num / den;
+      dv[j] = der / den;
+    }
+  }
+};
+
+static Lagrange1D closed_family(int p) { return Lagrange1D{gll_nodes(p)}; }
+static Lagrange1D open_family(int p) {  // degree p: p+1 Gauss points
+  std::vector<double> x, w;
+  gauss_rule(p + 1, x, w);
+  return Lagrange1D{x};
+}
+
+// ----------------------------------------------------------------------------
+// Reference bases: tabulate at points
+// ----------------------------------------------------------------------------
+
+// Scalar tensor Lagrange basis of degree p on [-1,1]^dim: per point, per dof,
+// out[(dof)*(1+dim) + 0] = value, + 1 + k = d/dxi_k.  Returns card.
+static int tab_hgrad(int dim, int p, const double* xi, double* out) {
+  Lagrange1D L = closed_family(p);
+  int m = L.n();
+  double v[3][32], dv[3][32];
+  for (int k = 0; k < dim; k++) L.eval(xi[k], v[k], dv[k]);
+  int card = 1;
+  for (int k = 0; k < dim; k++) card *= m;
+  for (int idx = 0; idx < card; idx++) {
+    int ii[3] = {idx % m, (idx / m) % m, idx / (m * m)};
+    double val = 1.0;
+    for (int k = 0; k < dim; k++) val *= v[k][ii[k]];
+    out[idx * (1 + dim)] = val;
+    for (int k = 0; k < dim; k++) {
+      double g = 1.0;
+      for (int j = 0; j < dim; j++) g *= (j == k) ? dv[j][ii[j]] : v[j][ii[j]];
+      out[idx * (1 + dim) + 1 + k] = g;
+    }
+  }
+  return card;
+}
+
+// Tensor Raviart-Thomas In: out[dof*(dim+1) + c] = value comp c, + dim = div.
+static int tab_hdiv(int dim, int n, const double* xi, double* out) {
+  Lagrange1D C = closed_family(n), O = open_family(n - 1);
+  double cv[3][32], cd[3][32], ov[3][32], od[3][32];
+  for (int k = 0; k < dim; k++) {
+    C.eval(xi[k], cv[k], cd[k]);
+    O.eval(xi[k], ov[k], od[k]);
+  }
+  int dof = 0;
+  for (int comp = 0; comp < dim; comp++) {
+    int ext[3];
+    for (int k = 0; k < dim; k++) ext[k] = (k == comp) ? C.n() : O.n();
+    int cnt = 1;
+    for (int k = 0; k < dim; k++) cnt *= ext[k];
+    for (int idx = 0; idx < cnt; idx++) {
+      int ii[3], r = idx;
+      for (int k = 0; k < dim; k++) { ii[k] = r % ext[k]; r /= ext[k]; }
+      double f = 1.0, df = 1.0;
+      for (int k = 0; k < dim; k++) {
+        double a = (k == comp) ? cv[k][ii[k]] : ov[k][ii[k]];
+        f *= a;
+        df *= (k == comp) ? cd[k][ii[k]] : a;
+      }
+      for (int c = 0; c < dim; c++) out[dof * (dim + 1) + c] = (c == comp) ? f : 0.0;
+      out[dof * (dim + 1) + dim] = df;
+      dof++;
+    }
+  }
+  return dof;
+}
+
+static int card_hgrad(int dim, int p) {
+  int m = p + 1, c = 1;
+  for (int k = 0; k < dim; k++) c *= m;
+  return c;
+}
+static int card_hdiv(int dim, int n) { return dim == 2 ? 2 * n * (n + 1) : 3 * n * n * (n + 1); }
+
+// ----------------------------------------------------------------------------
+// Topology data (shards)
+// ----------------------------------------------------------------------------
+
+struct TopoData {
+  int d, nv, ns;
+  double v[8][3];
+  int sv[6][4];
+};
+
+static bool topo_data(int key, TopoData& t) {
+  std::memset(&t, 0, sizeof(t));
+  if (key == DPG_TOPO_QUAD) {
+    t.d = 2; t.nv = 4; t.ns = 4;
+    const double v[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+    for (int a = 0; a < 4; a++) { t.v[a][0] = v[a][0]; t.v[a][1] = v[a][1]; }
+    for (int s = 0; s < 4; s++) { t.sv[s][0] = s; t.sv[s][1] = (s + 1) & 3; }
+    return true;
+  }
+  if (key == DPG_TOPO_HEX) {
+    t.d = 3; t.nv = 8; t.ns = 6;
+    for (int a = 0; a < 8; a++) {
+      int lo = a & 3;
+      t.v[a][0] = (lo == 1 || lo == 2) ? 1 : -1;
+      t.v[a][1] = (lo >= 2) ? 1 : -1;
+      t.v[a][2] = (a >= 4) ? 1 : -1;
+    }
+    const int f[6][4] = {{0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}, {0, 3, 2, 1}, {4, 5, 6, 7}};
+    std::memcpy(t.sv, f, sizeof(f));
+    return true;
+  }
+  return false;
+}
+
+// d(vertex shape)/d(xi) of the (bi/tri)linear geometric map
+static void geom_dshape(const TopoData& t, const double* xi, double* dN) {
+  for (int a = 0; a < t.nv; a++)
+    for (int k = 0; k < t.d; k++) {
+      double g = 0.5 * t.v[a][k];
+      for (int j = 0; j < t.d; j++)
+        if (j != k) g *= 0.5 * (1.0 + xi[j] * t.v[a][j]);
+      dN[a * t.d + k] = g;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Plan
+// ----------------------------------------------------------------------------
+
+static int pad8(int n) { return (n + 7) & ~7; }
+static int ld_pad(int n) {  // >= n, == 4 (mod 16): conflict-free fragment loads
+  int x = n;
+  while ((x & 15) != 4) x++;
+  return x;
+}
+
+struct HostPlan;
+
+static double* upload(HostPlan* P, const std::vector<double>& v);
+static int* upload_i(HostPlan* P, const std::vector<int>& v);
+
+struct HostPlan {
+  dpg_bucket_desc desc;
+  dpg_plan_info info;
+  DpgPlanDev dev;           // host copy with device pointers inside
+  DpgPlanDev* d_dev = nullptr;
+  std::vector<void*> allocs;
+  int device = 0;
+  // host staging for dpg_assemble_host
+  void* h_ws = nullptr;
+  size_t ws_bytes = 0;
+  void* d_ws = nullptr;
+  cudaStream_t streams[2] = {nullptr, nullptr};
+};
+
+static double* upload(HostPlan* P, const std::vector<double>& v) {
+  void* p = nullptr;
+  size_t bytes = std::max<size_t>(8, v.size() * sizeof(double));
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  if (!v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+  P->allocs.push_back(p);
+  return (double*)p;
+}
+static int* upload_i(HostPlan* P, const std::vector<int>& v) {
+  void* p = nullptr;
+  size_t bytes = std::max<size_t>(8, v.size() * sizeof(int));
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  if (!v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice);
+  P->allocs.push_back(p);
+  return (int*)p;
+}
+
+struct Rule {
+  std::vector<double> x, w;  // x: npts*dim
+  int n = 0;
+};
+
+static Rule tensor_rule(int dim, int degree) {
+  int n1 = degree / 2 + 1;
+  std::vector<double> x, w;
+  gauss_rule(n1, x, w);
+  Rule r;
+  r.n = 1;
+  for (int k = 0; k < dim; k++) r.n *= n1;
+  r.x.resize(r.n * dim);
+  r.w.resize(r.n);
+  for (int q = 0; q < r.n; q++) {
+    int rem = q;
+    double wt = 1.0;
+    for (int k = 0; k < dim; k++) {
+      int i = rem % n1;
+      rem /= n1;
+      r.x[q * dim + k] = x[i];
+      wt *= w[i];
+    }
+    r.w[q] = wt;
+  }
+  return r;
+}
+
+static int build(HostPlan* P, const dpg_bucket_desc* D) {
+  DpgPlanDev& g = P->dev;
+  std::memset(&g, 0, sizeof(g));
+  TopoData T;
+  if (D->topology == DPG_TOPO_TRI) return fail(DPG_ERR_UNSUPPORTED, "triangle buckets are not supported by this build");
+  if (!topo_data(D->topology, T)) return fail(DPG_ERR_INVALID_ARGUMENT, "unknown topology");
+  if (D->n_test < 1 || D->n_test > DPG_MAXV || D->n_trial < 1 || D->n_trial > DPG_MAXV)
+    return fail(DPG_ERR_UNSUPPORTED, "number of test/trial vars out of range (1..8)");
+  int d = T.d;
+  g.d = d; g.nv = T.nv; g.ns = T.ns;
+  g.nslots = D->n_slots;
+  Rule rG = tensor_rule(d, D->cub_degree_G), rB = tensor_rule(d, D->cub_degree_B),
+       rS = tensor_rule(d - 1, D->cub_degree_side);
+  g.QG = rG.n; g.QB = rB.n; g.QS = rS.n;
+  g.Ptot = g.QG + g.QB + g.ns * g.QS;
+  // side points in the volume reference cell, and reference tangents
+  std::vector<double> sidepts(g.ns * g.QS * d), sideT(g.ns * g.QS * 6, 0.0);
+  for (int s = 0; s < g.ns; s++)
+    for (int q = 0; q < g.QS; q++) {
+      double* X = &sidepts[(s * g.QS + q) * d];
+      double* Tq = &sideT[(s * g.QS + q) * 6];
+      if (d == 2) {
+        double t = rS.x[q];
+        const double* a = T.v[T.sv[s][0]];
+        const double* b = T.v[T.sv[s][1]];
+        for (int k = 0; k < 2; k++) {
+          X[k] = 0.5 * (1 - t) * a[k] + 0.5 * (1 + t) * b[k];
+          Tq[k] = 0.5 * (b[k] - a[k]);
+        }
+      } else {
+        double u = rS.x[q * 2], w = rS.x[q * 2 + 1];
+        double Nq[4] = {0.25 * (1 - u) * (1 - w), 0.25 * (1 + u) * (1 - w), 0.25 * (1 + u) * (1 + w),
+                        0.25 * (1 - u) * (1 + w)};
+        double Nu[4] = {-0.25 * (1 - w), 0.25 * (1 - w), 0.25 * (1 + w), -0.25 * (1 + w)};
+        double Nw[4] = {-0.25 * (1 - u), -0.25 * (1 + u), 0.25 * (1 + u), 0.25 * (1 - u)};
+        for (int k = 0; k < 3; k++) {
+          X[k] = 0; Tq[k] = 0; Tq[3 + k] = 0;
+          for (int a = 0; a < 4; a++) {
+            const double* V = T.v[T.sv[s][a]];
+            X[k] += Nq[a] * V[k];
+            Tq[k] += Nu[a] * V[k];
+            Tq[3 + k] += Nw[a] * V[k];
+          }
+        }
+      }
+    }
+  // geometry tables
+  std::vector<double> dNG(g.QG * T.nv * d), dNB(g.QB * T.nv * d), dNS(g.ns * g.QS * T.nv * d);
+  for (int q = 0; q < g.QG; q++) geom_dshape(T, &rG.x[q * d], &dNG[q * T.nv * d]);
+  for (int q = 0; q < g.QB; q++) geom_dshape(T, &rB.x[q * d], &dNB[q * T.nv * d]);
+  for (int q = 0; q < g.ns * g.QS; q++) geom_dshape(T, &sidepts[q * d], &dNS[q * T.nv * d]);
+
+  // ---- test vars ----------------------------------------------------------
+  int dev_row = 0, user_row = 0;
+  for (int a = 0; a < D->n_test; a++) {
+    const dpg_var_desc& V = D->test[a];
+    DpgTestVar& tv = g.test[a];
+    tv.space = V.space;
+    int n = V.poly_order;
+    if (V.space == DPG_SPACE_HGRAD) { tv.card = card_hgrad(d, n); tv.nref = 1 + d; }
+    else if (V.space == DPG_SPACE_HDIV) {
+      if (n < 1) return fail(DPG_ERR_INVALID_ARGUMENT, "HDIV test order must be >= 1");
+      tv.card = card_hdiv(d, n); tv.nref = d + 1;
+    } else return fail(DPG_ERR_INVALID_ARGUMENT, "test vars must be HGRAD or HDIV");
+    tv.dev_off = dev_row;
+    tv.user_off = user_row;
+    tv.ntile0 = dev_row / 8;
+    tv.ntiles = pad8(tv.card) / 8;
+    tv.ldA = ld_pad(pad8(tv.card));
+    dev_row += pad8(tv.card);
+    user_row += tv.card;
+    auto tab = [&](const double* pts, int npts) {
+      std::vector<double> out((size_t)npts * tv.card * tv.nref);
+      std::vector<double> tmp((size_t)tv.card * tv.nref);
+      for (int q = 0; q < npts; q++) {
+        if (V.space == DPG_SPACE_HGRAD) tab_hgrad(d, n, pts + q * d, tmp.data());
+        else tab_hdiv(d, n, pts + q * d, tmp.data());
+        std::copy(tmp.begin(), tmp.end(), out.begin() + (size_t)q * tv.card * tv.nref);
+      }
+      return out;
+    };
+    tv.tabG = upload(P, tab(rG.x.data(), g.QG));
+    tv.tabB = upload(P, tab(rB.x.data(), g.QB));
+    tv.tabS = upload(P, tab(sidepts.data(), g.ns * g.QS));
+  }
+  g.ntest = D->n_test;
+  g.N = user_row;
+  g.Np = dev_row;
+  g.NBT = g.Np / 8;
+  if (g.NBT > DPG_MAX_NBT)
+    return fail(DPG_ERR_UNSUPPORTED, "test space too large for the single-CTA kernel (N > 192 after padding)");
+
+  // ---- trial vars -----------------------------------------------------------
+  int nf = 0, ntr = 0, user_col = 0;
+  bool seen_trace = false;
+  for (int b = 0; b < D->n_trial; b++) {
+    const dpg_var_desc& V = D->trial[b];
+    if (V.kind == DPG_VAR_FIELD) {
+      if (seen_trace) return fail(DPG_ERR_UNSUPPORTED, "field vars must precede trace/flux vars");
+    } else seen_trace = true;
+  }
+  std::vector<int> user_of_dev;  // built below
+  int fcount = 0;
+  for (int b = 0; b < D->n_trial; b++) {
+    const dpg_var_desc& V = D->trial[b];
+    DpgTrialVar& tr = g.trial[b];
+    tr.kind = V.kind;
+    tr.space = V.space;
+    if (V.kind == DPG_VAR_FIELD) {
+      if (V.space != DPG_SPACE_HVOL && V.space != DPG_SPACE_VECTOR_HVOL)
+        return fail(DPG_ERR_INVALID_ARGUMENT, "field vars must be HVOL or VECTOR_HVOL");
+      int p = V.poly_order - 1;
+      if (p < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "field H1Order must be >= 1");
+      tr.ncomp = (V.space == DPG_SPACE_VECTOR_HVOL) ? d : 1;
+      tr.card_comp = card_hgrad(d, p);
+      tr.per_side = 0;
+      tr.user_off = user_col;
+      tr.dev_off = fcount;
+      fcount += tr.ncomp * tr.card_comp;
+      user_col += tr.ncomp * tr.card_comp;
+      std::vector<double> tb((size_t)g.QB * tr.card_comp), ts((size_t)g.ns * g.QS * tr.card_comp);
+      std::vector<double> tmp((size_t)tr.card_comp * (1 + d));
+      for (int q = 0; q < g.QB; q++) {
+        tab_hgrad(d, p, &rB.x[q * d], tmp.data());
+        for (int i = 0; i < tr.card_comp; i++) tb[(size_t)q * tr.card_comp + i] = tmp[i * (1 + d)];
+      }
+      for (int q = 0; q < g.ns * g.QS; q++) {
+        tab_hgrad(d, p, &sidepts[q * d], tmp.data());
+        for (int i = 0; i < tr.card_comp; i++) ts[(size_t)q * tr.card_comp + i] = tmp[i * (1 + d)];
+      }
+      tr.tabB = upload(P, tb);
+      tr.tabS = upload(P, ts);
+    } else if (V.kind == DPG_VAR_TRACE || V.kind == DPG_VAR_FLUX) {
+      int p = (V.space == DPG_SPACE_HGRAD) ? V.poly_order : V.poly_order - 1;
+      if (p < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "trace order must be >= 0");
+      tr.ncomp = 1;
+      tr.per_side = card_hgrad(d - 1, p);
+      tr.card_comp = tr.per_side;
+      tr.user_off = user_col;
+      user_col += tr.per_side * g.ns;
+      std::vector<double> ts((size_t)g.QS * tr.per_side), tmp((size_t)tr.per_side * d);
+      for (int q = 0; q < g.QS; q++) {
+        tab_hgrad(d - 1, p, &rS.x[q * (d - 1)], tmp.data());
+        for (int i = 0; i < tr.per_side; i++) ts[(size_t)q * tr.per_side + i] = tmp[i * d];
+      }
+      tr.tabS = upload(P, ts);
+      tr.tabB = nullptr;
+    } else {
+      return fail(DPG_ERR_INVALID_ARGUMENT, "trial var kind must be FIELD, TRACE or FLUX");
+    }
+  }
+  nf = fcount;
+  g.ntrial = D->n_trial;
+  g.M = user_col;
+  g.nf = nf;
+  g.nt = g.M - nf;
+  ntr = g.nt;
+  g.nfp = pad8(nf);
+  g.ntp = pad8(ntr);
+  g.nfb = g.nfp / 8;
+  g.fcol = g.nfp + g.ntp;
+  g.Mp = g.fcol + 8;
+  g.MBT = g.Mp / 8;
+  if (g.MBT > DPG_MAX_MBT)
+    return fail(DPG_ERR_UNSUPPORTED, "trial space too large for the single-CTA kernel (M > 120 after padding)");
+  // trace device offsets
+  {
+    int off = g.nfp;
+    for (int b = 0; b < D->n_trial; b++) {
+      DpgTrialVar& tr = g.trial[b];
+      if (tr.kind == DPG_VAR_FIELD) continue;
+      tr.dev_off = off;
+      off += tr.per_side * g.ns;
+    }
+  }
+  std::vector<int> d2u_trial(g.Mp, -1), d2u_test(g.Np, -1);
+  for (int b = 0; b < D->n_trial; b++) {
+    const DpgTrialVar& tr = g.trial[b];
+    int cnt = (tr.kind == DPG_VAR_FIELD) ? tr.ncomp * tr.card_comp : tr.per_side * g.ns;
+    for (int i = 0; i < cnt; i++) d2u_trial[tr.dev_off + i] = tr.user_off + i;
+  }
+  for (int a = 0; a < g.ntest; a++)
+    for (int i = 0; i < g.test[a].card; i++) d2u_test[g.test[a].dev_off + i] = g.test[a].user_off + i;
+  g.dev2user_trial = upload_i(P, d2u_trial);
+  g.dev2user_test = upload_i(P, d2u_test);
+
+  // ---- Gram features and IP entries ---------------------------------------
+  g.Ftot = 4 * g.ntest;
+  for (int a = 0; a < g.ntest; a++) g.test[a].nfeat = 0;
+  if (D->n_ip > DPG_MAX_IP) return fail(DPG_ERR_UNSUPPORTED, "too many IP entries");
+  int maxrow = 0;
+  std::map<std::pair<int, int>, int> rowid;
+  for (int e = 0; e < D->n_ip; e++) {
+    const dpg_ip_entry& E = D->ip[e];
+    if (E.test_var < 0 || E.test_var >= g.ntest) return fail(DPG_ERR_INVALID_ARGUMENT, "IP entry test var out of range");
+    DpgTestVar& tv = g.test[E.test_var];
+    int op = E.test_op;
+    bool ok = (tv.space == DPG_SPACE_HGRAD) ? (op == DPG_OP_VALUE || (op >= DPG_OP_DX && op < DPG_OP_DX + d))
+                                            : ((op >= DPG_OP_X && op < DPG_OP_X + d) || op == DPG_OP_DIV);
+    if (!ok) return fail(DPG_ERR_INVALID_ARGUMENT, "IP op not valid for the test var's space");
+    int k = -1;
+    for (int j = 0; j < tv.nfeat; j++)
+      if (tv.feat_op[j] == op) k = j;
+    if (k < 0) {
+      if (tv.nfeat >= 4) return fail(DPG_ERR_UNSUPPORTED, "more than 4 Gram features on one test var");
+      k = tv.nfeat++;
+      tv.feat_op[k] = op;
+    }
+    auto key = std::make_pair(E.term, E.comp);
+    if (!rowid.count(key)) {
+      int r = (int)rowid.size();
+      rowid[key] = r;
+    }
+    DpgIPEnt& I = g.ipent[e];
+    I.row = rowid[key];
+    I.gfeat = E.test_var * 4 + k;
+    I.coef = E.coef;
+    I.slot = E.slot;
+    if (E.slot >= D->n_slots) return fail(DPG_ERR_INVALID_ARGUMENT, "IP slot out of range");
+  }
+  g.nipent = D->n_ip;
+  g.niprows = (int)rowid.size();
+  if (g.niprows > DPG_MAX_IPROWS) return fail(DPG_ERR_UNSUPPORTED, "too many IP rows");
+  (void)maxrow;
+  // staged layout per point: features [var][4][ldA], h blocks [a][b<=a][4][ldA_b]
+  {
+    int off = 0;
+    std::vector<int> foff(g.ntest);
+    for (int a = 0; a < g.ntest; a++) { foff[a] = off; off += 4 * g.test[a].ldA; }
+    g.featstride = off;
+    off = 0;
+    for (int a = 0; a < g.ntest; a++)
+      for (int b = 0; b <= a; b++) { g.hoff[a][b] = off; off += 4 * g.test[b].ldA; }
+    g.hstride = off;
+    std::vector<DpgGTile> tiles;
+    for (int I = 0; I < g.NBT; I++)
+      for (int J = 0; J <= I; J++) {
+        int a = 0, b = 0;
+        for (int v = 0; v < g.ntest; v++) {
+          if (I >= g.test[v].ntile0 && I < g.test[v].ntile0 + g.test[v].ntiles) a = v;
+          if (J >= g.test[v].ntile0 && J < g.test[v].ntile0 + g.test[v].ntiles) b = v;
+        }
+        DpgGTile t;
+        t.I = I; t.J = J;
+        t.aoff = foff[a] + (I - g.test[a].ntile0) * 8;
+        t.lda = g.test[a].ldA;
+        t.boff = g.hoff[a][b] + (J - g.test[b].ntile0) * 8;
+        t.ldb = g.test[b].ldA;
+        tiles.push_back(t);
+      }
+    g.ngt = (int)tiles.size();
+    if ((g.ngt + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_GT) return fail(DPG_ERR_UNSUPPORTED, "too many G tiles");
+    void* p = nullptr;
+    if (cudaMalloc(&p, tiles.size() * sizeof(DpgGTile)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
+    cudaMemcpy(p, tiles.data(), tiles.size() * sizeof(DpgGTile), cudaMemcpyHostToDevice);
+    P->allocs.push_back(p);
+    g.gtiles = (const DpgGTile*)p;
+  }
+
+  // ---- B terms, segments, RHS ----------------------------------------------
+  if (D->n_bf + D->n_rhs > DPG_MAX_BF) return fail(DPG_ERR_UNSUPPORTED, "too many bilinear terms");
+  if (D->n_rhs > DPG_MAX_RHS) return fail(DPG_ERR_UNSUPPORTED, "too many RHS terms");
+  g.ldT = ld_pad(g.Mp);
+  std::vector<DpgBTerm> terms;
+  auto test_op_ok = [&](int a, int op, bool side) {
+    const DpgTestVar& tv = g.test[a];
+    if (tv.space == DPG_SPACE_HGRAD) return op == DPG_OP_VALUE || (op >= DPG_OP_DX && op < DPG_OP_DX + d);
+    return (op >= DPG_OP_X && op < DPG_OP_X + d) || op == DPG_OP_DIV || (side && op == DPG_OP_DOT_NORMAL);
+  };
+  for (int e = 0; e < D->n_bf; e++) {
+    const dpg_bf_term& B = D->bf[e];
+    if (B.trial_var < 0 || B.trial_var >= g.ntrial || B.test_var < 0 || B.test_var >= g.ntest)
+      return fail(DPG_ERR_INVALID_ARGUMENT, "bf term var index out of range");
+    if (B.slot >= D->n_slots) return fail(DPG_ERR_INVALID_ARGUMENT, "bf slot out of range");
+    const DpgTrialVar& tr = g.trial[B.trial_var];
+    if (!test_op_ok(B.test_var, B.test_op, B.boundary)) return fail(DPG_ERR_INVALID_ARGUMENT, "bf test op invalid");
+    if (tr.kind != DPG_VAR_FIELD && !B.boundary) return fail(DPG_ERR_INVALID_ARGUMENT, "trace/flux terms must be boundary terms");
+    if (B.normal_comp >= d) return fail(DPG_ERR_INVALID_ARGUMENT, "normal component out of range");
+    int comp = 0;
+    if (tr.kind == DPG_VAR_FIELD) {
+      if (tr.ncomp > 1) {
+        if (B.trial_op < DPG_OP_X || B.trial_op >= DPG_OP_X + d) return fail(DPG_ERR_INVALID_ARGUMENT, "vector field needs op X/Y/Z");
+        comp = B.trial_op - DPG_OP_X;
+      } else if (B.trial_op != DPG_OP_VALUE) return fail(DPG_ERR_INVALID_ARGUMENT, "scalar field needs op VALUE");
+    }
+    int nseg = B.boundary ? g.ns : 1;
+    for (int sg = 0; sg < nseg; sg++) {
+      DpgBTerm t;
+      std::memset(&t, 0, sizeof(t));
+      t.trial_var = B.trial_var; t.trial_op = B.trial_op; t.test_var = B.test_var; t.test_op = B.test_op;
+      t.coef = B.coef; t.slot = B.slot; t.normal_comp = B.normal_comp;
+      t.seg = B.boundary ? 1 + sg : 0;
+      t.kind = tr.kind;
+      t.tvar_comp = comp;
+      if (tr.kind == DPG_VAR_FIELD) { t.col0 = tr.dev_off + comp * tr.card_comp; t.ncol = tr.card_comp; }
+      else { t.col0 = tr.dev_off + sg * tr.per_side; t.ncol = tr.per_side; }
+      terms.push_back(t);
+    }
+  }
+  for (int e = 0; e < D->n_rhs; e++) {
+    const dpg_rhs_term& R = D->rhs[e];
+    if (R.test_var < 0 || R.test_var >= g.ntest || !test_op_ok(R.test_var, R.test_op, false))
+      return fail(DPG_ERR_INVALID_ARGUMENT, "rhs term invalid");
+    if (R.slot >= D->n_slots) return fail(DPG_ERR_INVALID_ARGUMENT, "rhs slot out of range");
+    DpgBTerm t;
+    std::memset(&t, 0, sizeof(t));
+    t.trial_var = -1; t.test_var = R.test_var; t.test_op = R.test_op;
+    t.coef = R.coef; t.slot = R.slot; t.normal_comp = -1; t.seg = 0; t.kind = -1;
+    t.col0 = g.fcol; t.ncol = 1;
+    terms.push_back(t);
+  }
+  std::stable_sort(terms.begin(), terms.end(), [](const DpgBTerm& x, const DpgBTerm& y) { return x.seg < y.seg; });
+  if ((int)terms.size() > DPG_MAX_BF) return fail(DPG_ERR_UNSUPPORTED, "too many expanded bilinear terms");
+  g.nseg = 1 + g.ns;
+  for (int sg = 0; sg < g.nseg; sg++) {
+    DpgSeg& S = g.seg[sg];
+    S.npts = sg == 0 ? g.QB : g.QS;
+    S.nops = 0;
+    S.term0 = -1;
+    S.nterm = 0;
+    int off = 0;
+    for (int i = 0; i < (int)terms.size(); i++) {
+      DpgBTerm& t = terms[i];
+      if (t.seg != sg) continue;
+      if (S.term0 < 0) S.term0 = i;
+      S.nterm++;
+      int k = -1;
+      for (int j = 0; j < S.nops; j++)
+        if (S.ops[j].var == t.test_var && S.ops[j].op == t.test_op) k = j;
+      if (k < 0) {
+        if (S.nops >= DPG_MAX_BOPS) return fail(DPG_ERR_UNSUPPORTED, "too many test ops in a segment");
+        k = S.nops++;
+        S.ops[k].var = t.test_var;
+        S.ops[k].op = t.test_op;
+        S.ops[k].off = off;
+        off += DPG_CHUNK * g.test[t.test_var].ldA;
+      }
+      t.bop = k;
+    }
+    if (S.term0 < 0) S.term0 = 0;
+    S.opstride = off;
+  }
+  g.nbterm = (int)terms.size();
+  for (int i = 0; i < g.nbterm; i++) g.bterm[i] = terms[i];
+
+  // ---- geometry uploads ------------------------------------------------------
+  g.dNG = upload(P, dNG);
+  g.dNB = upload(P, dNB);
+  g.dNS = upload(P, dNS);
+  g.wG = upload(P, rG.w);
+  g.wB = upload(P, rB.w);
+  g.wS = upload(P, rS.w);
+  g.sideT = upload(P, sideT);
+
+  // ---- shared memory layout (doubles) ----------------------------------------
+  {
+    int geo = DPG_CHUNK * 32;
+    int cm = DPG_CHUNK * g.Ftot * g.Ftot + DPG_CHUNK * DPG_MAX_IPROWS * g.Ftot;
+    int gphase = geo + cm + DPG_CHUNK * g.featstride + DPG_CHUNK * g.hstride;
+    g.sm_geo = 0;
+    g.sm_cmat = geo;
+    g.sm_feat = geo + cm;
+    g.sm_h = g.sm_feat + DPG_CHUNK * g.featstride;
+    g.sm_gt = 0;
+    int gt = g.ngt * 64;
+    g.sm_linv = gt;
+    g.sm_scale = g.sm_linv + g.NBT * 64;
+    int geo2 = g.sm_scale + g.Np;
+    // B phase: geometry of the chunk, staged ops, staged trial values
+    int maxops = 0, maxterm = 0;
+    for (int sg = 0; sg < g.nseg; sg++) {
+      maxops = std::max(maxops, g.seg[sg].opstride);
+      maxterm = std::max(maxterm, g.seg[sg].nterm);
+    }
+    g.sm_misc = geo2;                       // chunk geometry for the B phase (DPG_CHUNK * 32)
+    g.sm_bops = g.sm_misc + DPG_CHUNK * 32;
+    g.sm_bval = g.sm_bops + maxops;
+    int bphase = g.sm_bval + maxterm * DPG_CHUNK * g.ldT;
+    g.sm_w = 0;
+    int wsz = g.MBT * g.NBT * 64;
+    g.sm_k = 0;
+    int ksz = g.MBT * (g.MBT + 1) / 2 * 64;
+    int total = std::max(std::max(gphase, bphase), std::max(wsz, ksz));
+    g.sm_total = total + 64;  // + cell nodes / flags
+    if ((size_t)g.sm_total * 8 > 232448)
+      return fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
+  }
+  // info
+  dpg_plan_info& I = P->info;
+  I.N = g.N; I.M = g.M; I.n_field = g.nf; I.n_trace = g.nt;
+  I.space_dim = d; I.n_vertices = T.nv; I.n_sides = T.ns;
+  I.Q_G = g.QG; I.Q_B = g.QB; I.Q_side = g.QS; I.n_points_total = g.Ptot;
+  I.n_slots = g.nslots; I.precision = D->precision;
+  // device copy of the plan
+  void* p = nullptr;
+  if (cudaMalloc(&p, sizeof(DpgPlanDev)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc plan");
+  cudaMemcpy(p, &g, sizeof(DpgPlanDev), cudaMemcpyHostToDevice);
+  P->allocs.push_back(p);
+  P->d_dev = (DpgPlanDev*)p;
+  for (void* a : P->allocs)
+    if (!a) return fail(DPG_ERR_OUT_OF_MEMORY, "device table allocation failed");
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return fail(DPG_ERR_CUDA, std::string("plan upload: ") + cudaGetErrorString(err));
+  return DPG_OK;
+}
+
+}  // namespace dpg
+
+// Plan of the bare optimal-test solve (TBF::factoredCholeskySolve): one test
+// block of N rows, M trial columns treated as fields (no condensation).
+int dpg_make_solve_plan(int N, int M, DpgPlanDev* out) {
+  DpgPlanDev& g = *out;
+  std::memset(&g, 0, sizeof(g));
+  auto pad8 = [](int n) { return (n + 7) & ~7; };
+  g.d = 2; g.nv = 0; g.ns = 0;
+  g.N = N; g.M = M; g.nf = M; g.nt = 0;
+  g.Np = pad8(N); g.NBT = g.Np / 8;
+  g.nfp = pad8(M); g.ntp = 0; g.nfb = g.nfp / 8; g.fcol = g.nfp; g.Mp = g.nfp + 8; g.MBT = g.Mp / 8;
+  if (g.NBT > DPG_MAX_NBT) return dpg::fail(DPG_ERR_UNSUPPORTED, "N too large for the single-CTA solve (N <= 192)");
+  if (g.MBT > DPG_MAX_MBT) return dpg::fail(DPG_ERR_UNSUPPORTED, "M too large for the single-CTA solve (M <= 120)");
+  g.ntest = 1;
+  g.test[0].card = N; g.test[0].ntiles = g.NBT;
+  g.ntrial = 1;
+  g.trial[0].kind = DPG_VAR_FIELD; g.trial[0].ncomp = 1; g.trial[0].card_comp = M;
+  g.ngt = g.NBT * (g.NBT + 1) / 2;
+  g.sm_gt = 0;
+  g.sm_linv = g.ngt * 64;
+  g.sm_scale = g.sm_linv + g.NBT * 64;
+  int a = g.sm_scale + g.Np;
+  int w = g.MBT * g.NBT * 64, k = g.MBT * (g.MBT + 1) / 2 * 64;
+  g.sm_w = 0; g.sm_k = 0;
+  g.sm_total = std::max(a, std::max(w, k)) + 64;
+  return DPG_OK;
+}
+
+// Host-buffer pipeline: cells go through device memory in chunks on two
+// streams so that the copies of one chunk overlap the kernel of the other.
+int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d_ws, size_t* ws_bytes,
+                      cudaStream_t* streams, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                      double* K, double* l, double* S, double* s, int32_t* info, int flags) {
+  const DpgPlanDev& g = *plan;
+  if (C < 0) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!nodes || !parity || !info) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "nodes, parity and info are required");
+  if (g.nslots > 0 && !coeff) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+  bool wantK = !(flags & DPG_FLAG_NO_K), wantS = !(flags & DPG_FLAG_NO_CONDENSE);
+  if (wantK && (!K || !l)) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "K and l required");
+  if (wantS && (!S || !s)) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "S and s required");
+  const size_t nb_nodes = (size_t)g.nv * g.d * 8, nb_par = (size_t)g.ns, nb_co = (size_t)g.nslots * g.Ptot * 8;
+  const size_t nb_K = wantK ? (size_t)g.M * g.M * 8 : 0, nb_l = wantK ? (size_t)g.M * 8 : 0;
+  const size_t nb_S = wantS ? (size_t)g.nt * g.nt * 8 : 0, nb_s = wantS ? (size_t)g.nt * 8 : 0;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const int chunk = std::min(C, 4096);
+  const size_t per_buf = al(chunk * nb_nodes) + al(chunk * nb_par) + al(chunk * nb_co) + al(chunk * nb_K) +
+                         al(chunk * nb_l) + al(chunk * nb_S) + al(chunk * nb_s) + al(chunk * 4);
+  if (*ws_bytes < 2 * per_buf) {
+    if (*d_ws) cudaFree(*d_ws);
+    *d_ws = nullptr;
+    *ws_bytes = 0;
+    if (cudaMalloc(d_ws, 2 * per_buf) != cudaSuccess) {
+      cudaGetLastError();
+      return dpg::fail(DPG_ERR_OUT_OF_MEMORY, "workspace allocation failed");
+    }
+    *ws_bytes = 2 * per_buf;
+  }
+  for (int i = 0; i < 2; i++)
+    if (!streams[i] && cudaStreamCreateWithFlags(&streams[i], cudaStreamNonBlocking) != cudaSuccess)
+      return dpg::fail(DPG_ERR_CUDA, "stream creation failed");
+  for (int c0 = 0, it = 0; c0 < C; c0 += chunk, it++) {
+    const int n = std::min(chunk, C - c0);
+    const int b = it & 1;
+    cudaStream_t st = streams[b];
+    char* base = (char*)*d_ws + b * per_buf;
+    double* dn = (double*)base; base += al(chunk * nb_nodes);
+    int8_t* dp = (int8_t*)base; base += al(chunk * nb_par);
+    double* dc = (double*)base; base += al(chunk * nb_co);
+    double* dK = (double*)base; base += al(chunk * nb_K);
+    double* dl = (double*)base; base += al(chunk * nb_l);
+    double* dS = (double*)base; base += al(chunk * nb_S);
+    double* ds = (double*)base; base += al(chunk * nb_s);
+    int32_t* di = (int32_t*)base;
+    cudaMemcpyAsync(dn, (const char*)nodes + c0 * nb_nodes, n * nb_nodes, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dp, parity + (size_t)c0 * g.ns, n * nb_par, cudaMemcpyHostToDevice, st);
+    if (nb_co) cudaMemcpyAsync(dc, (const char*)coeff + c0 * nb_co, n * nb_co, cudaMemcpyHostToDevice, st);
+    DpgLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.C = n; L.nodes = dn; L.parity = dp; L.coeff = nb_co ? dc : nullptr;
+    L.K = wantK ? dK : nullptr; L.l = wantK ? dl : nullptr;
+    L.S = wantS ? dS : nullptr; L.s = wantS ? ds : nullptr;
+    L.info = di;
+    int rc = dpg_launch_assemble(plan, d_plan, &L, st);
+    if (rc != DPG_OK) return rc;
+    if (wantK) {
+      cudaMemcpyAsync((char*)K + c0 * nb_K, dK, n * nb_K, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync((char*)l + c0 * nb_l, dl, n * nb_l, cudaMemcpyDeviceToHost, st);
+    }
+    if (wantS) {
+      cudaMemcpyAsync((char*)S + c0 * nb_S, dS, n * nb_S, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync((char*)s + c0 * nb_s, ds, n * nb_s, cudaMemcpyDeviceToHost, st);
+    }
+    cudaMemcpyAsync(info + c0, di, n * 4, cudaMemcpyDeviceToHost, st);
+  }
+  cudaError_t e1 = cudaStreamSynchronize(streams[0]);
+  cudaError_t e2 = cudaStreamSynchronize(streams[1]);
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return dpg::fail(DPG_ERR_CUDA, std::string("host pipeline: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+  return DPG_OK;
+}
+
+// ============================================================================
+// C ABI
+// ============================================================================
+
+using namespace dpg;
+
+struct dpg_plan {
+  HostPlan hp;
+};
+
+extern "C" {
+
+const char* dpg_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* dpg_version(void) { return "camellia2_b200 dpg 1 (sm_100a, FP64 DMMA)"; }
+
+int dpg_plan_create(const dpg_bucket_desc* desc, dpg_plan** out) {
+  if (!desc || !out) return fail(DPG_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (desc->abi_version != DPG_ABI_VERSION) return fail(DPG_ERR_INVALID_ARGUMENT, "ABI version mismatch");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(DPG_ERR_CUDA, "no CUDA device available");
+  }
+  dpg_plan* p = new dpg_plan();
+  p->hp.desc = *desc;
+  cudaGetDevice(&p->hp.device);
+  int rc = build(&p->hp, desc);
+  if (rc != DPG_OK) {
+    std::string msg = g_last_error;
+    dpg_plan_destroy(p);
+    g_last_error = msg;
+    return rc;
+  }
+  rc = dpg_configure_kernels(&p->hp.dev);
+  if (rc != DPG_OK) {
+    std::string msg = g_last_error;
+    dpg_plan_destroy(p);
+    g_last_error = msg;
+    return rc;
+  }
+  *out = p;
+  return DPG_OK;
+}
+
+int dpg_plan_destroy(dpg_plan* p) {
+  if (!p) return DPG_OK;
+  for (void* a : p->hp.allocs)
+    if (a) cudaFree(a);
+  if (p->hp.d_ws) cudaFree(p->hp.d_ws);
+  for (auto& s : p->hp.streams)
+    if (s) cudaStreamDestroy(s);
+  delete p;
+  return DPG_OK;
+}
+
+int dpg_plan_query(const dpg_plan* p, dpg_plan_info* info) {
+  if (!p || !info) return fail(DPG_ERR_INVALID_ARGUMENT, "null argument");
+  *info = p->hp.info;
+  return DPG_OK;
+}
+
+int dpg_assemble(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff, double* K,
+                 double* l, double* S, double* s, int32_t* info, void* stream, int flags) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!nodes || !parity || !info) return fail(DPG_ERR_INVALID_ARGUMENT, "nodes, parity and info are required");
+  if (p->hp.dev.nslots > 0 && !coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+  if (!(flags & DPG_FLAG_NO_K) && (!K || !l)) return fail(DPG_ERR_INVALID_ARGUMENT, "K and l required");
+  if (!(flags & DPG_FLAG_NO_CONDENSE) && (!S || !s)) return fail(DPG_ERR_INVALID_ARGUMENT, "S and s required");
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.nodes = nodes; L.parity = parity; L.coeff = coeff;
+  L.K = (flags & DPG_FLAG_NO_K) ? nullptr : K;
+  L.l = (flags & DPG_FLAG_NO_K) ? nullptr : l;
+  L.S = (flags & DPG_FLAG_NO_CONDENSE) ? nullptr : S;
+  L.s = (flags & DPG_FLAG_NO_CONDENSE) ? nullptr : s;
+  L.info = info;
+  return dpg_launch_assemble(&p->hp.dev, p->hp.d_dev, &L, (cudaStream_t)stream);
+}
+
+int dpg_assemble_parts(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff, double* G,
+                       double* B, double* F, void* stream) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!nodes || !parity) return fail(DPG_ERR_INVALID_ARGUMENT, "nodes and parity are required");
+  if (p->hp.dev.nslots > 0 && !coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.nodes = nodes; L.parity = parity; L.coeff = coeff;
+  L.G = G; L.B = B; L.F = F;
+  L.parts = 1;
+  return dpg_launch_assemble(&p->hp.dev, p->hp.d_dev, &L, (cudaStream_t)stream);
+}
+
+int dpg_assemble_host(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff, double* K,
+                      double* l, double* S, double* s, int32_t* info, int flags) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  return dpg_host_pipeline(&p->hp.dev, p->hp.d_dev, &p->hp.d_ws, &p->hp.ws_bytes, p->hp.streams, C, nodes, parity,
+                           coeff, K, l, S, s, info, flags);
+}
+
+int dpg_factored_cholesky_solve(int C, int N, int M, const double* G, const double* B, const double* F, double* K,
+                                double* l, int32_t* info, void* stream) {
+  if (C < 0 || N <= 0 || M <= 0) return fail(DPG_ERR_INVALID_ARGUMENT, "bad sizes");
+  if (C == 0) return DPG_OK;
+  if (!G || !B || !F || !K || !l || !info) return fail(DPG_ERR_INVALID_ARGUMENT, "null argument");
+  DpgPlanDev P;
+  int rc = dpg_make_solve_plan(N, M, &P);
+  if (rc != DPG_OK) return rc;
+  rc = dpg_configure_kernels(&P);
+  if (rc != DPG_OK) return rc;
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.solve_only = 1; L.Gin = G; L.Bin = B; L.Fin = F; L.K = K; L.l = l; L.info = info;
+  return dpg_launch_assemble(&P, nullptr, &L, (cudaStream_t)stream);
+}
+
+int dpg_assemble_adjoint(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                         const double* Kbar, const double* lbar, double* coeff_bar, int32_t* info, void* stream) {
+  (void)p; (void)C; (void)nodes; (void)parity; (void)coeff; (void)Kbar; (void)lbar; (void)coeff_bar; (void)info;
+  (void)stream;
+  return fail(DPG_ERR_UNSUPPORTED, "adjoint not built yet");
+}
+
+int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags) {
+  for (int i = 0; i < n_buckets; i++) {
+    const dpg_bucket_batch& b = buckets[i];
+    int rc = dpg_assemble(b.plan, b.C, b.nodes, b.parity, b.coeff, b.K, b.l, b.S, b.s, b.info, stream, flags);
+    if (rc != DPG_OK) return rc;
+  }
+  return DPG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,42 @@
+// dpg_internal.h — declarations shared by the host builder and the kernel launchers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "dpg_plan.h"
+
+namespace dpg {
+extern thread_local std::string g_last_error;
+int fail(int code, const std::string& msg);
+}  // namespace dpg
+
+// Arguments of one assembly launch (device pointers).
+struct DpgLaunch {
+  int C;
+  const double* nodes;
+  const int8_t* parity;
+  const double* coeff;
+  double* K;
+  double* l;
+  double* S;
+  double* s;
+  int32_t* info;
+  // dpg_assemble_parts outputs (parts = 1): G (C,N,N), B (C,M,N), F (C,N)
+  int parts;
+  double* G;
+  double* B;
+  double* F;
+  // dpg_factored_cholesky_solve inputs (solve_only = 1)
+  int solve_only;
+  const double* Gin;
+  const double* Bin;
+  const double* Fin;
+};
+
+int dpg_configure_kernels(const DpgPlanDev* plan);
+int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const DpgLaunch* L, cudaStream_t stream);
+int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d_ws, size_t* ws_bytes,
+                      cudaStream_t* streams, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                      double* K, double* l, double* S, double* s, int32_t* info, int flags);
+int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);

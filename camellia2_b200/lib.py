@@ -1,0 +1,169 @@
+"""ctypes binding of libdpg_b200.so (the C ABI in include/dpg_b200.h).
+
+This is the host-side mirror of the reference's local-stiffness interface:
+``Plan.localStiffnessMatrixAndRHS`` returns what TBF::localStiffnessMatrixAndRHS
+(BF.cpp:1309-1496) returns, ``Plan.interpretLocalData``-style condensed outputs
+come from the same launch, ``factoredCholeskySolve`` mirrors
+TBF::factoredCholeskySolve (BF.cpp:924-1018).  torch is used only to hold
+device memory and streams.  There is no CPU fallback: if the library cannot be
+loaded or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdpg_b200.so")
+_LIB = None
+
+EXPORTED = [
+    "dpg_plan_create", "dpg_plan_destroy", "dpg_plan_query", "dpg_assemble", "dpg_assemble_host",
+    "dpg_assemble_parts", "dpg_factored_cholesky_solve", "dpg_assemble_adjoint", "dpg_assemble_multi",
+    "dpg_last_error_string", "dpg_version",
+]
+
+
+class DpgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dpg error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load the CUDA library (raises if it is missing: there is no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m camellia2_b200.build`")
+    L = ct.CDLL(LIB_PATH)
+    vp, i, d = ct.c_void_p, ct.c_int, ct.c_double
+    L.dpg_plan_create.argtypes = [vp, ct.POINTER(vp)]
+    L.dpg_plan_destroy.argtypes = [vp]
+    L.dpg_plan_query.argtypes = [vp, vp]
+    L.dpg_assemble.argtypes = [vp, i] + [vp] * 8 + [vp, i]
+    L.dpg_assemble_host.argtypes = [vp, i] + [vp] * 8 + [i]
+    L.dpg_assemble_parts.argtypes = [vp, i] + [vp] * 6 + [vp]
+    L.dpg_factored_cholesky_solve.argtypes = [i, i, i] + [vp] * 6 + [vp]
+    L.dpg_assemble_adjoint.argtypes = [vp, i] + [vp] * 7 + [vp]
+    L.dpg_assemble_multi.argtypes = [i, vp, vp, i]
+    L.dpg_last_error_string.restype = ct.c_char_p
+    L.dpg_version.restype = ct.c_char_p
+    _LIB = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise DpgError(rc, load().dpg_last_error_string().decode())
+
+
+def _ptr(x):
+    """Device or host address of a torch tensor / numpy array (None -> NULL)."""
+    if x is None:
+        return None
+    if hasattr(x, "data_ptr"):
+        return ct.c_void_p(x.data_ptr())
+    return x.ctypes.data_as(ct.c_void_p)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ct.c_void_p(stream.cuda_stream)
+
+
+class Plan:
+    """One bucket (Camellia ElementType) compiled for the GPU."""
+
+    def __init__(self, bucket):
+        self.holder = getattr(bucket, "holder", bucket)
+        L = load()
+        h = ct.c_void_p()
+        _check(L.dpg_plan_create(self.holder.ptr(), ct.byref(h)))
+        self.h = h
+        info = abi.PlanInfo()
+        _check(L.dpg_plan_query(self.h, ct.byref(info)))
+        self.info = info.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().dpg_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ device
+    def alloc_outputs(self, C, device="cuda"):
+        import torch
+        i = self.info
+        M, t = i["M"], i["n_trace"]
+        f64 = dict(dtype=torch.float64, device=device)
+        return dict(K=torch.empty((C, M, M), **f64), l=torch.empty((C, M), **f64),
+                    S=torch.empty((C, t, t), **f64), s=torch.empty((C, t), **f64),
+                    info=torch.empty((C,), dtype=torch.int32, device=device))
+
+    def assemble(self, nodes, parity, coeff=None, out=None, stream=None, flags=0):
+        """Device tensors in, device tensors out (asynchronous on `stream`)."""
+        C = nodes.shape[0]
+        if out is None:
+            out = self.alloc_outputs(C, nodes.device)
+        _check(load().dpg_assemble(self.h, C, _ptr(nodes), _ptr(parity), _ptr(coeff), _ptr(out["K"]),
+                                   _ptr(out["l"]), _ptr(out["S"]), _ptr(out["s"]), _ptr(out["info"]),
+                                   _stream_ptr(stream), flags))
+        return out
+
+    def localStiffnessMatrixAndRHS(self, nodes, parity, coeff=None):
+        o = self.assemble(nodes, parity, coeff)
+        return o["K"], o["l"]
+
+    def parts(self, nodes, parity, coeff=None, stream=None):
+        import torch
+        C = nodes.shape[0]
+        i = self.info
+        N, M = i["N"], i["M"]
+        f64 = dict(dtype=torch.float64, device=nodes.device)
+        G = torch.zeros((C, N, N), **f64)
+        B = torch.zeros((C, M, N), **f64)
+        F = torch.zeros((C, N), **f64)
+        _check(load().dpg_assemble_parts(self.h, C, _ptr(nodes), _ptr(parity), _ptr(coeff), _ptr(G), _ptr(B),
+                                         _ptr(F), _stream_ptr(stream)))
+        return G, B, F
+
+    # -------------------------------------------------------------------- host
+    def assemble_host(self, nodes, parity, coeff=None, out=None, flags=0):
+        """Host arrays (numpy or CPU torch, pinned is fastest) in and out."""
+        C = nodes.shape[0]
+        i = self.info
+        M, t = i["M"], i["n_trace"]
+        if out is None:
+            out = dict(K=np.empty((C, M, M)), l=np.empty((C, M)), S=np.empty((C, t, t)), s=np.empty((C, t)),
+                       info=np.empty((C,), dtype=np.int32))
+        _check(load().dpg_assemble_host(self.h, C, _ptr(nodes), _ptr(parity), _ptr(coeff), _ptr(out["K"]),
+                                        _ptr(out["l"]), _ptr(out["S"]), _ptr(out["s"]), _ptr(out["info"]), flags))
+        return out
+
+
+def factoredCholeskySolve(G, B, F, stream=None):
+    """Batched TBF::factoredCholeskySolve on device tensors G (C,N,N), B (C,M,N), F (C,N).
+    Returns K (C,M,M), l (C,M), info (C,)."""
+    import torch
+    C, N, _ = G.shape
+    M = B.shape[1]
+    K = torch.empty((C, M, M), dtype=torch.float64, device=G.device)
+    l = torch.empty((C, M), dtype=torch.float64, device=G.device)
+    info = torch.empty((C,), dtype=torch.int32, device=G.device)
+    _check(load().dpg_factored_cholesky_solve(C, N, M, _ptr(G.contiguous()), _ptr(B.contiguous()),
+                                              _ptr(F.contiguous()), _ptr(K), _ptr(l), _ptr(info),
+                                              _stream_ptr(stream)))
+    return K, l, info

@@ -1,0 +1,81 @@
+"""Synthetic meshes, side parities and per-point coefficients for the DPG
+assembly workloads (seeded numpy PCG64 streams).
+
+Vertex order per cell follows the shards topologies the reference uses
+(quad: counter-clockwise from (-1,-1); hex: bottom face counter-clockwise,
+then top face).  Side parities follow GlobalDofAssignment.cpp:158-258: a side
+shared by two cells is +1 on the cell with the lower cell ID and -1 on the
+other; boundary sides are +1.  Cell IDs are lexicographic, x fastest.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def quad_grid(nx, ny, jitter=0.0, seed=1, extent=(1.0, 1.0)):
+    """nx*ny quads on [0,Lx]x[0,Ly]; interior nodes jittered by U[-jitter*h, jitter*h]
+    per coordinate. Returns nodes (C,4,2) float64 and parity (C,4) int8."""
+    rng = np.random.default_rng(seed)
+    hx, hy = extent[0] / nx, extent[1] / ny
+    X, Y = np.meshgrid(np.arange(nx + 1) * hx, np.arange(ny + 1) * hy, indexing="ij")
+    if jitter:
+        jx = rng.uniform(-jitter * hx, jitter * hx, size=X.shape)
+        jy = rng.uniform(-jitter * hy, jitter * hy, size=Y.shape)
+        interior = np.zeros_like(X, dtype=bool)
+        interior[1:-1, 1:-1] = True
+        X = X + np.where(interior, jx, 0.0)
+        Y = Y + np.where(interior, jy, 0.0)
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")  # cell id = i + nx*j
+    i = i.reshape(-1)
+    j = j.reshape(-1)
+    corners = [(i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1)]
+    nodes = np.stack([np.stack([X[a, b], Y[a, b]], axis=-1) for a, b in corners], axis=1)
+    par = np.ones((nx * ny, 4), dtype=np.int8)
+    par[:, 0] = np.where(j > 0, -1, 1)       # bottom neighbour has the lower id
+    par[:, 3] = np.where(i > 0, -1, 1)       # left neighbour has the lower id
+    return np.ascontiguousarray(nodes), par
+
+
+def hex_grid(nx, ny, nz, jitter=0.0, seed=1, extent=(1.0, 1.0, 1.0)):
+    """nx*ny*nz hexes; interior nodes jittered by U[-jitter*h, jitter*h].
+    Returns nodes (C,8,3) float64 and parity (C,6) int8."""
+    rng = np.random.default_rng(seed)
+    h = [extent[0] / nx, extent[1] / ny, extent[2] / nz]
+    G = np.stack(np.meshgrid(np.arange(nx + 1) * h[0], np.arange(ny + 1) * h[1], np.arange(nz + 1) * h[2],
+                             indexing="ij"), axis=-1)
+    if jitter:
+        jit = np.stack([rng.uniform(-jitter * h[k], jitter * h[k], size=G.shape[:3]) for k in range(3)], axis=-1)
+        interior = np.zeros(G.shape[:3], dtype=bool)
+        interior[1:-1, 1:-1, 1:-1] = True
+        G = G + np.where(interior[..., None], jit, 0.0)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.reshape(-1), j.reshape(-1), k.reshape(-1)  # cell id = i + nx*(j + ny*k)
+    off = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    nodes = np.stack([G[i + a, j + b, k + c] for a, b, c in off], axis=1)
+    par = np.ones((nx * ny * nz, 6), dtype=np.int8)
+    par[:, 0] = np.where(j > 0, -1, 1)  # face y-
+    par[:, 3] = np.where(i > 0, -1, 1)  # face x-
+    par[:, 4] = np.where(k > 0, -1, 1)  # face z-
+    return np.ascontiguousarray(nodes), par
+
+
+def uniform_coeff(C, n_slots, n_points, low=-1.0, high=1.0, seed=1):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(low, high, size=(C, n_slots, n_points))
+
+
+def cdr_coeff(C, info, seed=1):
+    """Coefficients of the CDR workload: eps = exp(N(-4,1)) per point (slot 0 holds
+    sqrt(eps)), beta = (cos t, sin t) with t ~ U[0,2pi) per cell, alpha = c ~ U[0,1],
+    f ~ U[-1,1] per point."""
+    rng = np.random.default_rng(seed)
+    P = info["n_points_total"]
+    co = np.empty((C, 5, P))
+    eps = np.exp(rng.normal(-4.0, 1.0, size=(C, P)))
+    theta = rng.uniform(0.0, 2 * np.pi, size=(C, 1))
+    co[:, 0] = np.sqrt(eps)
+    co[:, 1] = np.cos(theta)
+    co[:, 2] = np.sin(theta)
+    co[:, 3] = rng.uniform(0.0, 1.0, size=(C, P))
+    co[:, 4] = rng.uniform(-1.0, 1.0, size=(C, P))
+    return co

@@ -1,0 +1,246 @@
+/*
+ * dpg_b200.h — C ABI of the B200-native DPG per-cell assembly library.
+ *
+ * One call assembles, for a batch of cells of ONE element type (Camellia's
+ * ElementType: topology + trial ordering + test ordering), the optimal-test
+ * local stiffness K = B^T G^-1 B, the load l = B^T G^-1 F, and the static
+ * condensation of the field dofs S = K_tt - K_ft^T K_ff^-1 K_ft,
+ * s = l_t - K_ft^T K_ff^-1 l_f.  Everything runs as hand-written sm_100a CUDA.
+ *
+ * Conventions shared by every entry point:
+ *   - every function returns an int status (DPG_OK = 0); no exception crosses
+ *     the boundary; dpg_last_error_string() describes the last failure on
+ *     the calling thread;
+ *   - all numbers are IEEE FP64, row-major, C-contiguous, one block per cell:
+ *       K  (C, M, M)   l (C, M)   S (C, t, t)   s (C, t)
+ *       G  (C, N, N)   B (C, M, N)  [Camellia's "stiffnessEnriched" layout]
+ *       F  (C, N)
+ *     N = test dofs, M = trial dofs, f = field dofs, t = M - f trace dofs;
+ *   - trial dofs are numbered var by var in the order of the trial list
+ *     (volume vars: all basis dofs; trace/flux vars: side 0 dofs, side 1
+ *     dofs, ...), exactly like Camellia's DofOrderingFactory::trialOrdering;
+ *     test dofs likewise in test-list order;
+ *   - numerical failures (a Gram matrix that is not positive definite) are
+ *     NOT errors: they are reported per cell in info[c] (0 = ok, k > 0 = the
+ *     leading minor of order k is not positive, as LAPACK DPOTRF's INFO;
+ *     -k = the condensation block failed at column k) and the call returns
+ *     DPG_OK, mirroring BF.cpp's printed-and-returned INFO.
+ *
+ * Reference interfaces replaced (paths inside ApolloFramework/camellia2):
+ *   dpg_plan_create           ElementType + BasisCache set-up for a bucket
+ *                             (src/Solution/Solution.cpp:1162-1187,
+ *                              src/Basis/BasisCache.cpp:236-267)
+ *   dpg_assemble              TBF::localStiffnessMatrixAndRHS, FACTORED_CHOLESKY
+ *                             (src/ScratchPad/BF.cpp:1309-1496) followed by
+ *                             CondensedDofInterpreter::interpretLocalData
+ *                             (src/Solution/CondensedDofInterpreter.cpp:1063-1225)
+ *   dpg_assemble_host         the same, host buffers in and out
+ *   dpg_assemble_parts        TIP::computeInnerProductMatrix (src/ScratchPad/IP.cpp:215-292),
+ *                             TBF::stiffnessMatrix rowMajor=true (src/ScratchPad/BF.cpp:575-656),
+ *                             TRHS::integrateAgainstStandardBasis (src/Problem/RHS.cpp:68-82)
+ *   dpg_factored_cholesky_solve  TBF::factoredCholeskySolve (src/ScratchPad/BF.cpp:924-1018)
+ *   dpg_assemble_adjoint      no counterpart in the reference (new capability)
+ */
+#ifndef DPG_B200_H
+#define DPG_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPG_ABI_VERSION 1
+
+/* status codes */
+#define DPG_OK 0
+#define DPG_ERR_INVALID_ARGUMENT 1
+#define DPG_ERR_UNSUPPORTED 2
+#define DPG_ERR_CUDA 3
+#define DPG_ERR_OUT_OF_MEMORY 4
+#define DPG_ERR_TIMEOUT 5
+#define DPG_ERR_BAD_PLAN 6
+
+/* cell topologies (shards keys in the reference) */
+#define DPG_TOPO_QUAD 1
+#define DPG_TOPO_HEX 2
+#define DPG_TOPO_TRI 3
+
+/* function spaces (Camellia::Space / EFunctionSpace) */
+#define DPG_SPACE_HGRAD 1
+#define DPG_SPACE_HDIV 2
+#define DPG_SPACE_HVOL 3        /* L2 */
+#define DPG_SPACE_VECTOR_HVOL 4 /* VECTOR_L2, component-major dofs */
+
+/* variable kinds (Camellia::VarType) */
+#define DPG_VAR_FIELD 1
+#define DPG_VAR_TRACE 2
+#define DPG_VAR_FLUX 3 /* trace whose values are multiplied by the side parity */
+#define DPG_VAR_TEST 4
+
+/* operators (Camellia::EOperator subset) */
+#define DPG_OP_VALUE 0
+#define DPG_OP_X 1 /* vector component x (HDIV test, VECTOR_HVOL field) */
+#define DPG_OP_Y 2
+#define DPG_OP_Z 3
+#define DPG_OP_DX 4 /* gradient components of an HGRAD test function */
+#define DPG_OP_DY 5
+#define DPG_OP_DZ 6
+#define DPG_OP_DIV 7
+#define DPG_OP_DOT_NORMAL 8 /* tau . n on a side */
+
+/* precision of the quadrature contractions */
+#define DPG_PREC_FP64 0
+#define DPG_PREC_MIXED 1 /* split-precision tensor-core contractions, FP64 factor/solve */
+
+/* dpg_assemble flags */
+#define DPG_FLAG_NO_K 1        /* do not write K / l (condensed outputs only) */
+#define DPG_FLAG_NO_CONDENSE 2 /* do not write S / s */
+
+typedef struct dpg_var_desc {
+  int kind;       /* DPG_VAR_* */
+  int space;      /* DPG_SPACE_* */
+  int poly_order; /* Camellia H1Order of the variable (test: k + delta_k) */
+} dpg_var_desc;
+
+/* One scalar product in a bilinear term:
+ *   coef * slot(x) * [n_{normal_comp}] * trialOp(u) * testOp(v)
+ * integrated over the cell volume (boundary = 0) or over every side
+ * (boundary = 1).  Vector dot products are expanded into components. */
+typedef struct dpg_bf_term {
+  int trial_var;   /* index into the trial list */
+  int trial_op;    /* DPG_OP_VALUE, or DPG_OP_X/Y/Z for a VECTOR_HVOL field */
+  int test_var;    /* index into the test list */
+  int test_op;     /* DPG_OP_* */
+  double coef;
+  int slot;        /* coefficient slot, or -1 */
+  int normal_comp; /* -1, or 0..2: also multiply by the outward unit normal's component */
+  int boundary;    /* 0: volume integral, 1: sum of side integrals */
+} dpg_bf_term;
+
+/* One summand of the inner product (graph norm): term `term`, component
+ * `comp` of the vector-valued linear term L_term gets coef*slot*op(v).
+ * G = sum_term sum_comp  integral  L_{term,comp}(v_i) L_{term,comp}(v_j). */
+typedef struct dpg_ip_entry {
+  int term;
+  int comp;
+  int test_var;
+  int test_op;
+  double coef;
+  int slot;
+} dpg_ip_entry;
+
+/* One summand of the load: F_i = integral coef * slot(x) * op(v_i) */
+typedef struct dpg_rhs_term {
+  int test_var;
+  int test_op;
+  double coef;
+  int slot;
+} dpg_rhs_term;
+
+typedef struct dpg_bucket_desc {
+  int abi_version; /* DPG_ABI_VERSION */
+  int topology;    /* DPG_TOPO_* */
+  int n_trial;
+  const dpg_var_desc* trial;
+  int n_test;
+  const dpg_var_desc* test;
+  int n_bf;
+  const dpg_bf_term* bf;
+  int n_ip;
+  const dpg_ip_entry* ip;
+  int n_rhs;
+  const dpg_rhs_term* rhs;
+  int cub_degree_G;    /* Gram (testVsTest) rule degree: 2 * max test degree */
+  int cub_degree_B;    /* volume rule for B and F: max trial + max test degree */
+  int cub_degree_side; /* side rule: max trace degree + max test degree */
+  int n_slots;         /* number of per-point coefficient slots */
+  int precision;       /* DPG_PREC_* */
+} dpg_bucket_desc;
+
+/* Sizes a caller needs to size its buffers. Coefficients are laid out
+ * coeff[c][slot][p] with p over n_points_total = Q_G + Q_B + n_sides * Q_side
+ * (Gram-rule volume points, then B-rule volume points, then side points
+ * side-major).  Point order inside a tensor rule is x fastest. */
+typedef struct dpg_plan_info {
+  int N, M, n_field, n_trace;
+  int space_dim, n_vertices, n_sides;
+  int Q_G, Q_B, Q_side, n_points_total;
+  int n_slots;
+  int precision;
+} dpg_plan_info;
+
+typedef struct dpg_plan dpg_plan;
+
+/* Build the per-bucket plan: basis and weight tables at the cubature points,
+ * the compiled term lists and the launch configuration. Device tables are
+ * created on the current CUDA device. */
+int dpg_plan_create(const dpg_bucket_desc* desc, dpg_plan** plan);
+int dpg_plan_destroy(dpg_plan* plan);
+int dpg_plan_query(const dpg_plan* plan, dpg_plan_info* info);
+
+/* Assemble C cells; all pointers are DEVICE pointers.
+ *   nodes  (C, n_vertices, space_dim)   physical vertex coordinates
+ *   parity (C, n_sides) int8 +-1        Camellia cellSideParities
+ *   coeff  (C, n_slots, n_points_total) may be NULL when n_slots == 0
+ *   K, l, S, s as above (K/l may be NULL with DPG_FLAG_NO_K, S/s with
+ *   DPG_FLAG_NO_CONDENSE); info (C) int32.
+ * stream: a cudaStream_t (NULL = legacy default stream). Asynchronous. */
+int dpg_assemble(dpg_plan* plan, int C, const double* nodes, const int8_t* parity,
+                 const double* coeff, double* K, double* l, double* S, double* s,
+                 int32_t* info, void* stream, int flags);
+
+/* Same as dpg_assemble with HOST buffers (pinned memory is fastest). The
+ * library stages the cells through device memory in chunks with copies
+ * overlapped with compute; returns after the results are in host memory. */
+int dpg_assemble_host(dpg_plan* plan, int C, const double* nodes, const int8_t* parity,
+                      const double* coeff, double* K, double* l, double* S, double* s,
+                      int32_t* info, int flags);
+
+/* The quadrature products alone (device pointers; any output may be NULL). */
+int dpg_assemble_parts(dpg_plan* plan, int C, const double* nodes, const int8_t* parity,
+                       const double* coeff, double* G, double* B, double* F, void* stream);
+
+/* Batched factored-Cholesky optimal-test solve on given matrices (device
+ * pointers). G (C,N,N) symmetric, B (C,M,N) [column-major N x M per cell],
+ * F (C,N). Outputs K (C,M,M), l (C,M), info (C). Inputs are not modified. */
+int dpg_factored_cholesky_solve(int C, int N, int M, const double* G, const double* B,
+                                const double* F, double* K, double* l, int32_t* info,
+                                void* stream);
+
+/* Adjoint of dpg_assemble (K and l outputs) for a loss J(K, l):
+ * given Kbar (C,M,M) and lbar (C,M) = dJ/dK, dJ/dl, writes
+ * coeff_bar (C, n_slots, n_points_total) = dJ/dcoeff. Device pointers. */
+int dpg_assemble_adjoint(dpg_plan* plan, int C, const double* nodes, const int8_t* parity,
+                         const double* coeff, const double* Kbar, const double* lbar,
+                         double* coeff_bar, int32_t* info, void* stream);
+
+/* Multi-bucket assembly: one persistent launch walks a work queue over
+ * several plans' cell ranges. Pointers per bucket as in dpg_assemble. */
+typedef struct dpg_bucket_batch {
+  dpg_plan* plan;
+  int C;
+  const double* nodes;
+  const int8_t* parity;
+  const double* coeff;
+  double* K;
+  double* l;
+  double* S;
+  double* s;
+  int32_t* info;
+} dpg_bucket_batch;
+
+int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags);
+
+/* Thread-local description of the last error. */
+const char* dpg_last_error_string(void);
+
+/* Library version string and the compiled architecture. */
+const char* dpg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DPG_B200_H */

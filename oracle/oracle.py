@@ -1,0 +1,146 @@
+"""ctypes binding of the CPU oracle (oracle/dpg_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the camellia2_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+from camellia2_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build():
+    subprocess.check_call(["bash", os.path.join(_HERE, "build.sh")])
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ct.CDLL(path)
+        L.orc_plan_create.restype = ct.c_void_p
+        L.orc_plan_create.argtypes = [ct.c_void_p]
+        L.orc_plan_destroy.argtypes = [ct.c_void_p]
+        L.orc_plan_query.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.orc_assemble.argtypes = [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 11 + [ct.c_int]
+        L.orc_factored_cholesky_solve.argtypes = [ct.c_int, ct.c_int] + [ct.c_void_p] * 5
+        L.orc_condense.argtypes = [ct.c_int] + [ct.c_void_p] * 5
+        L.orc_trial_is_field.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.orc_basis_tabulate.argtypes = [ct.c_int] * 4 + [ct.c_void_p] * 4
+        L.orc_cubature.argtypes = [ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p]
+        L.orc_last_error.restype = ct.c_char_p
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+class OraclePlan:
+    def __init__(self, bucket_or_holder):
+        holder = getattr(bucket_or_holder, "holder", bucket_or_holder)
+        self.holder = holder
+        self.h = lib().orc_plan_create(holder.ptr())
+        if not self.h:
+            raise RuntimeError("oracle plan: " + lib().orc_last_error().decode())
+        info = abi.PlanInfo()
+        lib().orc_plan_query(self.h, ct.byref(info))
+        self.info = info.as_dict()
+        self.is_field = np.zeros(self.info["M"], dtype=np.int32)
+        lib().orc_trial_is_field(self.h, _p(self.is_field))
+
+    def __del__(self):
+        try:
+            lib().orc_plan_destroy(self.h)
+        except Exception:
+            pass
+
+    def assemble(self, nodes, parity, coeff=None, parts=False, nthreads=1):
+        i = self.info
+        C = nodes.shape[0]
+        N, M, t = i["N"], i["M"], i["n_trace"]
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        parity = np.ascontiguousarray(parity, dtype=np.int8)
+        if coeff is not None:
+            coeff = np.ascontiguousarray(coeff, dtype=np.float64)
+        out = {}
+        if parts:
+            out["G"] = np.zeros((C, N, N))
+            out["B"] = np.zeros((C, M, N))
+            out["F"] = np.zeros((C, N))
+        out["K"] = np.zeros((C, M, M))
+        out["l"] = np.zeros((C, M))
+        out["S"] = np.zeros((C, t, t))
+        out["s"] = np.zeros((C, t))
+        out["info"] = np.zeros(C, dtype=np.int32)
+        lib().orc_assemble(self.h, C, _p(nodes), _p(parity), _p(coeff), _p(out.get("G")), _p(out.get("B")),
+                           _p(out.get("F")), _p(out["K"]), _p(out["l"]), _p(out["S"]), _p(out["s"]),
+                           _p(out["info"]), nthreads)
+        return out
+
+    def parts(self, nodes, parity, coeff=None):
+        i = self.info
+        C = nodes.shape[0]
+        N, M = i["N"], i["M"]
+        G, B, F = np.zeros((C, N, N)), np.zeros((C, M, N)), np.zeros((C, N))
+        lib().orc_assemble(self.h, C, _p(np.ascontiguousarray(nodes, dtype=np.float64)),
+                           _p(np.ascontiguousarray(parity, dtype=np.int8)),
+                           _p(None if coeff is None else np.ascontiguousarray(coeff, dtype=np.float64)),
+                           _p(G), _p(B), _p(F), None, None, None, None, None, 1)
+        return G, B, F
+
+
+def factored_cholesky_solve(G, B, F):
+    """Single cell: G (N,N), B (M,N) [stiffnessEnriched layout], F (N)."""
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    F = np.ascontiguousarray(F, dtype=np.float64)
+    N, M = G.shape[0], B.shape[0]
+    K, l = np.zeros((M, M)), np.zeros(M)
+    info = lib().orc_factored_cholesky_solve(N, M, _p(G), _p(B), _p(F), _p(K), _p(l))
+    return K, l, info
+
+
+def condense(is_field, K, l):
+    is_field = np.ascontiguousarray(is_field, dtype=np.int32)
+    K = np.ascontiguousarray(K, dtype=np.float64)
+    l = np.ascontiguousarray(l, dtype=np.float64)
+    t = int((is_field == 0).sum())
+    S, s = np.zeros((t, t)), np.zeros(t)
+    err = lib().orc_condense(K.shape[0], _p(is_field), _p(K), _p(l), _p(S), _p(s))
+    return S, s, err
+
+
+def basis_tabulate(topo, space, n, pts):
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    npts = pts.shape[0]
+    # size generously, then trim
+    big = 4096
+    d = pts.shape[1]
+    val = np.zeros((npts, big * d))
+    grad = np.zeros((npts, big * d))
+    div = np.zeros((npts, big))
+    card = lib().orc_basis_tabulate(topo, space, n, npts, _p(pts), _p(val), _p(grad), _p(div))
+    vdim = d if space == abi.SPACE_HDIV else 1
+    flat_v = val.reshape(-1)[: npts * card * vdim].reshape(npts, card, vdim)
+    flat_g = grad.reshape(-1)[: npts * card * d].reshape(npts, card, d)
+    flat_d = div.reshape(-1)[: npts * card].reshape(npts, card)
+    return flat_v, flat_g, flat_d
+
+
+def cubature(dim, degree):
+    n = (degree // 2 + 1) ** dim
+    pts, wts = np.zeros((n, dim)), np.zeros(n)
+    lib().orc_cubature(dim, degree, _p(pts), _p(wts))
+    return pts, wts
