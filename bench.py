@@ -313,9 +313,9 @@ def main():
                        "cells": C, "form": "fp64", "l2": "no flush: each step reads 0.15 GB and writes 16.3 GB "
                                                           "(> 126 MB L2)",
                        "parallelism": f"{world} GPU(s), cells sharded (weak), no data-path collective"},
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "flops_per_cell": fl, "peak_source": "measured live: torch float64 GEMM 8192^3"},
+                         "flops_per_cell": fl, "peak_source": "measured live: torch float64 GEMM 8192^3 (DMMA d884), FP64 tensor pipe"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
