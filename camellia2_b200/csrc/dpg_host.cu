@@ -321,19 +321,25 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   if (!topo_data(D->topology, T)) return fail(DPG_ERR_INVALID_ARGUMENT, "unknown topology");
   if (D->n_test < 1 || D->n_test > DPG_MAXV || D->n_trial < 1 || D->n_trial > DPG_MAXV)
     return fail(DPG_ERR_UNSUPPORTED, "number of test/trial vars out of range (1..8)");
-  int d = T.d;
+  const int d = T.d;
   g.d = d; g.nv = T.nv; g.ns = T.ns;
   g.nslots = D->n_slots;
   Rule rG = tensor_rule(d, D->cub_degree_G), rB = tensor_rule(d, D->cub_degree_B),
        rS = tensor_rule(d - 1, D->cub_degree_side);
   g.QG = rG.n; g.QB = rB.n; g.QS = rS.n;
+  if (g.QG > DPG_MAX_QG) return fail(DPG_ERR_UNSUPPORTED, "Gram cubature rule too large");
+  auto padc = [](int n, int c) { return (n + c - 1) / c * c; };
+  g.QGpad = padc(g.QG, DPG_CHG);
+  g.QBpad = padc(g.QB, 8);
+  g.QSpad = padc(g.QS, 8);
   g.Ptot = g.QG + g.QB + g.ns * g.QS;
-  // side points in the volume reference cell, and reference tangents
-  std::vector<double> sidepts(g.ns * g.QS * d), sideT(g.ns * g.QS * 6, 0.0);
+  // side points in the volume reference cell and reference tangents (padded per side)
+  std::vector<double> sidepts((size_t)g.ns * g.QSpad * d), sideT((size_t)g.ns * g.QSpad * 6, 0.0);
   for (int s = 0; s < g.ns; s++)
-    for (int q = 0; q < g.QS; q++) {
-      double* X = &sidepts[(s * g.QS + q) * d];
-      double* Tq = &sideT[(s * g.QS + q) * 6];
+    for (int qq = 0; qq < g.QSpad; qq++) {
+      const int q = qq < g.QS ? qq : 0;  // padding repeats point 0 (weight 0)
+      double* X = &sidepts[((size_t)s * g.QSpad + qq) * d];
+      double* Tq = &sideT[((size_t)s * g.QSpad + qq) * 6];
       if (d == 2) {
         double t = rS.x[q];
         const double* a = T.v[T.sv[s][0]];
@@ -359,63 +365,86 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
         }
       }
     }
-  // geometry tables
-  std::vector<double> dNG(g.QG * T.nv * d), dNB(g.QB * T.nv * d), dNS(g.ns * g.QS * T.nv * d);
-  for (int q = 0; q < g.QG; q++) geom_dshape(T, &rG.x[q * d], &dNG[q * T.nv * d]);
-  for (int q = 0; q < g.QB; q++) geom_dshape(T, &rB.x[q * d], &dNB[q * T.nv * d]);
-  for (int q = 0; q < g.ns * g.QS; q++) geom_dshape(T, &sidepts[q * d], &dNS[q * T.nv * d]);
+  // padded volume point lists (padding repeats point 0 with weight 0)
+  auto pad_pts = [&](const Rule& r, int npad, std::vector<double>& x, std::vector<double>& w) {
+    x.assign((size_t)npad * d, 0.0);
+    w.assign(npad, 0.0);
+    for (int q = 0; q < npad; q++) {
+      int src = q < r.n ? q : 0;
+      for (int k = 0; k < d; k++) x[(size_t)q * d + k] = r.x[(size_t)src * d + k];
+      w[q] = q < r.n ? r.w[q] : 0.0;
+    }
+  };
+  std::vector<double> xG, wG, xB, wB;
+  pad_pts(rG, g.QGpad, xG, wG);
+  pad_pts(rB, g.QBpad, xB, wB);
+  std::vector<double> wS(g.QSpad, 0.0);
+  for (int q = 0; q < g.QS; q++) wS[q] = rS.w[q];
+  auto dshape = [&](const std::vector<double>& x, int n) {
+    std::vector<double> out((size_t)n * T.nv * d);
+    for (int q = 0; q < n; q++) geom_dshape(T, &x[(size_t)q * d], &out[(size_t)q * T.nv * d]);
+    return out;
+  };
 
   // ---- test vars ----------------------------------------------------------
-  int dev_row = 0, user_row = 0;
+  int dev_row = 0, user_row = 0, foff = 0;
+  std::vector<int> test_n(D->n_test);
   for (int a = 0; a < D->n_test; a++) {
     const dpg_var_desc& V = D->test[a];
     DpgTestVar& tv = g.test[a];
     tv.space = V.space;
     int n = V.poly_order;
-    if (V.space == DPG_SPACE_HGRAD) { tv.card = card_hgrad(d, n); tv.nref = 1 + d; }
+    test_n[a] = n;
+    if (V.space == DPG_SPACE_HGRAD) tv.card = card_hgrad(d, n);
     else if (V.space == DPG_SPACE_HDIV) {
       if (n < 1) return fail(DPG_ERR_INVALID_ARGUMENT, "HDIV test order must be >= 1");
-      tv.card = card_hdiv(d, n); tv.nref = d + 1;
+      tv.card = card_hdiv(d, n);
     } else return fail(DPG_ERR_INVALID_ARGUMENT, "test vars must be HGRAD or HDIV");
     tv.dev_off = dev_row;
     tv.user_off = user_row;
     tv.ntile0 = dev_row / 8;
     tv.ntiles = pad8(tv.card) / 8;
     tv.ldA = ld_pad(pad8(tv.card));
+    tv.foff = foff;
+    foff += 4 * tv.ldA;
     dev_row += pad8(tv.card);
     user_row += tv.card;
-    auto tab = [&](const double* pts, int npts) {
-      std::vector<double> out((size_t)npts * tv.card * tv.nref);
-      std::vector<double> tmp((size_t)tv.card * tv.nref);
-      for (int q = 0; q < npts; q++) {
-        if (V.space == DPG_SPACE_HGRAD) tab_hgrad(d, n, pts + q * d, tmp.data());
-        else tab_hdiv(d, n, pts + q * d, tmp.data());
-        std::copy(tmp.begin(), tmp.end(), out.begin() + (size_t)q * tv.card * tv.nref);
-      }
-      return out;
-    };
-    tv.tabG = upload(P, tab(rG.x.data(), g.QG));
-    tv.tabB = upload(P, tab(rB.x.data(), g.QB));
-    tv.tabS = upload(P, tab(sidepts.data(), g.ns * g.QS));
   }
   g.ntest = D->n_test;
+  g.featstride = foff;
   g.N = user_row;
   g.Np = dev_row;
   g.NBT = g.Np / 8;
   if (g.NBT > DPG_MAX_NBT)
     return fail(DPG_ERR_UNSUPPORTED, "test space too large for the single-CTA kernel (N > 192 after padding)");
+  // staged reference slots of all test vars at a list of volume-reference points
+  auto fref_table = [&](const double* pts, int npts) {
+    std::vector<double> out((size_t)npts * g.featstride, 0.0);
+    for (int q = 0; q < npts; q++)
+      for (int a = 0; a < g.ntest; a++) {
+        const DpgTestVar& tv = g.test[a];
+        std::vector<double> tmp((size_t)tv.card * (d + 1));
+        if (tv.space == DPG_SPACE_HGRAD) tab_hgrad(d, test_n[a], pts + (size_t)q * d, tmp.data());
+        else tab_hdiv(d, test_n[a], pts + (size_t)q * d, tmp.data());
+        double* dst = &out[(size_t)q * g.featstride + tv.foff];
+        for (int i = 0; i < tv.card; i++)
+          for (int m = 0; m <= d; m++) dst[(size_t)m * tv.ldA + i] = tmp[(size_t)i * (d + 1) + m];
+      }
+    return out;
+  };
+  g.frefG = upload(P, fref_table(xG.data(), g.QGpad));
+  g.wG = upload(P, wG);
+  g.dNG = upload(P, dshape(xG, g.QGpad));
 
   // ---- trial vars -----------------------------------------------------------
-  int nf = 0, ntr = 0, user_col = 0;
   bool seen_trace = false;
   for (int b = 0; b < D->n_trial; b++) {
-    const dpg_var_desc& V = D->trial[b];
-    if (V.kind == DPG_VAR_FIELD) {
+    if (D->trial[b].kind == DPG_VAR_FIELD) {
       if (seen_trace) return fail(DPG_ERR_UNSUPPORTED, "field vars must precede trace/flux vars");
     } else seen_trace = true;
   }
-  std::vector<int> user_of_dev;  // built below
-  int fcount = 0;
+  int fcount = 0, user_col = 0;
+  std::vector<std::vector<double>> host_tabB(D->n_trial), host_tabS(D->n_trial);
   for (int b = 0; b < D->n_trial; b++) {
     const dpg_var_desc& V = D->trial[b];
     DpgTrialVar& tr = g.trial[b];
@@ -428,23 +457,24 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       if (p < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "field H1Order must be >= 1");
       tr.ncomp = (V.space == DPG_SPACE_VECTOR_HVOL) ? d : 1;
       tr.card_comp = card_hgrad(d, p);
-      tr.per_side = 0;
       tr.user_off = user_col;
       tr.dev_off = fcount;
       fcount += tr.ncomp * tr.card_comp;
       user_col += tr.ncomp * tr.card_comp;
-      std::vector<double> tb((size_t)g.QB * tr.card_comp), ts((size_t)g.ns * g.QS * tr.card_comp);
+      std::vector<double> tb((size_t)g.QBpad * tr.card_comp), ts((size_t)g.ns * g.QSpad * tr.card_comp);
       std::vector<double> tmp((size_t)tr.card_comp * (1 + d));
-      for (int q = 0; q < g.QB; q++) {
-        tab_hgrad(d, p, &rB.x[q * d], tmp.data());
-        for (int i = 0; i < tr.card_comp; i++) tb[(size_t)q * tr.card_comp + i] = tmp[i * (1 + d)];
+      for (int q = 0; q < g.QBpad; q++) {
+        tab_hgrad(d, p, &xB[(size_t)q * d], tmp.data());
+        for (int i = 0; i < tr.card_comp; i++) tb[(size_t)q * tr.card_comp + i] = tmp[(size_t)i * (1 + d)];
       }
-      for (int q = 0; q < g.ns * g.QS; q++) {
-        tab_hgrad(d, p, &sidepts[q * d], tmp.data());
-        for (int i = 0; i < tr.card_comp; i++) ts[(size_t)q * tr.card_comp + i] = tmp[i * (1 + d)];
+      for (int q = 0; q < g.ns * g.QSpad; q++) {
+        tab_hgrad(d, p, &sidepts[(size_t)q * d], tmp.data());
+        for (int i = 0; i < tr.card_comp; i++) ts[(size_t)q * tr.card_comp + i] = tmp[(size_t)i * (1 + d)];
       }
       tr.tabB = upload(P, tb);
       tr.tabS = upload(P, ts);
+      host_tabB[b] = tb;
+      host_tabS[b] = ts;
     } else if (V.kind == DPG_VAR_TRACE || V.kind == DPG_VAR_FLUX) {
       int p = (V.space == DPG_SPACE_HGRAD) ? V.poly_order : V.poly_order - 1;
       if (p < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "trace order must be >= 0");
@@ -453,32 +483,31 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       tr.card_comp = tr.per_side;
       tr.user_off = user_col;
       user_col += tr.per_side * g.ns;
-      std::vector<double> ts((size_t)g.QS * tr.per_side), tmp((size_t)tr.per_side * d);
-      for (int q = 0; q < g.QS; q++) {
-        tab_hgrad(d - 1, p, &rS.x[q * (d - 1)], tmp.data());
-        for (int i = 0; i < tr.per_side; i++) ts[(size_t)q * tr.per_side + i] = tmp[i * d];
+      std::vector<double> ts((size_t)g.QSpad * tr.per_side), tmp((size_t)tr.per_side * d);
+      for (int qq = 0; qq < g.QSpad; qq++) {
+        int q = qq < g.QS ? qq : 0;
+        tab_hgrad(d - 1, p, &rS.x[(size_t)q * (d - 1)], tmp.data());
+        for (int i = 0; i < tr.per_side; i++) ts[(size_t)qq * tr.per_side + i] = tmp[(size_t)i * d];
       }
       tr.tabS = upload(P, ts);
       tr.tabB = nullptr;
+      host_tabS[b] = ts;
     } else {
       return fail(DPG_ERR_INVALID_ARGUMENT, "trial var kind must be FIELD, TRACE or FLUX");
     }
   }
-  nf = fcount;
   g.ntrial = D->n_trial;
   g.M = user_col;
-  g.nf = nf;
-  g.nt = g.M - nf;
-  ntr = g.nt;
-  g.nfp = pad8(nf);
-  g.ntp = pad8(ntr);
+  g.nf = fcount;
+  g.nt = g.M - fcount;
+  g.nfp = pad8(g.nf);
+  g.ntp = pad8(g.nt);
   g.nfb = g.nfp / 8;
   g.fcol = g.nfp + g.ntp;
   g.Mp = g.fcol + 8;
   g.MBT = g.Mp / 8;
   if (g.MBT > DPG_MAX_MBT)
     return fail(DPG_ERR_UNSUPPORTED, "trial space too large for the single-CTA kernel (M > 120 after padding)");
-  // trace device offsets
   {
     int off = g.nfp;
     for (int b = 0; b < D->n_trial; b++) {
@@ -499,28 +528,26 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   g.dev2user_trial = upload_i(P, d2u_trial);
   g.dev2user_test = upload_i(P, d2u_test);
 
-  // ---- Gram features and IP entries ---------------------------------------
-  g.Ftot = 4 * g.ntest;
-  for (int a = 0; a < g.ntest; a++) g.test[a].nfeat = 0;
+  // ---- Gram: IP entries on physical slots ----------------------------------
   if (D->n_ip > DPG_MAX_IP) return fail(DPG_ERR_UNSUPPORTED, "too many IP entries");
-  int maxrow = 0;
   std::map<std::pair<int, int>, int> rowid;
+  auto phys_slot = [&](int a, int op) -> int {
+    const DpgTestVar& tv = g.test[a];
+    if (tv.space == DPG_SPACE_HGRAD) {
+      if (op == DPG_OP_VALUE) return 0;
+      if (op >= DPG_OP_DX && op < DPG_OP_DX + d) return 1 + (op - DPG_OP_DX);
+      return -1;
+    }
+    if (op >= DPG_OP_X && op < DPG_OP_X + d) return op - DPG_OP_X;
+    if (op == DPG_OP_DIV) return d;
+    return -1;
+  };
   for (int e = 0; e < D->n_ip; e++) {
     const dpg_ip_entry& E = D->ip[e];
     if (E.test_var < 0 || E.test_var >= g.ntest) return fail(DPG_ERR_INVALID_ARGUMENT, "IP entry test var out of range");
-    DpgTestVar& tv = g.test[E.test_var];
-    int op = E.test_op;
-    bool ok = (tv.space == DPG_SPACE_HGRAD) ? (op == DPG_OP_VALUE || (op >= DPG_OP_DX && op < DPG_OP_DX + d))
-                                            : ((op >= DPG_OP_X && op < DPG_OP_X + d) || op == DPG_OP_DIV);
-    if (!ok) return fail(DPG_ERR_INVALID_ARGUMENT, "IP op not valid for the test var's space");
-    int k = -1;
-    for (int j = 0; j < tv.nfeat; j++)
-      if (tv.feat_op[j] == op) k = j;
-    if (k < 0) {
-      if (tv.nfeat >= 4) return fail(DPG_ERR_UNSUPPORTED, "more than 4 Gram features on one test var");
-      k = tv.nfeat++;
-      tv.feat_op[k] = op;
-    }
+    int sl = phys_slot(E.test_var, E.test_op);
+    if (sl < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "IP op not valid for the test var's space");
+    if (E.slot >= D->n_slots) return fail(DPG_ERR_INVALID_ARGUMENT, "IP slot out of range");
     auto key = std::make_pair(E.term, E.comp);
     if (!rowid.count(key)) {
       int r = (int)rowid.size();
@@ -528,25 +555,29 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     }
     DpgIPEnt& I = g.ipent[e];
     I.row = rowid[key];
-    I.gfeat = E.test_var * 4 + k;
+    I.gslot = E.test_var * 4 + sl;
     I.coef = E.coef;
     I.slot = E.slot;
-    if (E.slot >= D->n_slots) return fail(DPG_ERR_INVALID_ARGUMENT, "IP slot out of range");
   }
   g.nipent = D->n_ip;
+  std::stable_sort(g.ipent, g.ipent + g.nipent, [](const DpgIPEnt& x, const DpgIPEnt& y) { return x.row < y.row; });
   g.niprows = (int)rowid.size();
   if (g.niprows > DPG_MAX_IPROWS) return fail(DPG_ERR_UNSUPPORTED, "too many IP rows");
-  (void)maxrow;
-  // staged layout per point: features [var][4][ldA], h blocks [a][b<=a][4][ldA_b]
+  // var pairs (a >= b), h block offsets
   {
-    int off = 0;
-    std::vector<int> foff(g.ntest);
-    for (int a = 0; a < g.ntest; a++) { foff[a] = off; off += 4 * g.test[a].ldA; }
-    g.featstride = off;
-    off = 0;
+    int off = 0, np = 0;
     for (int a = 0; a < g.ntest; a++)
-      for (int b = 0; b <= a; b++) { g.hoff[a][b] = off; off += 4 * g.test[b].ldA; }
+      for (int b = 0; b <= a; b++) {
+        if (np >= DPG_MAX_PAIRS) return fail(DPG_ERR_UNSUPPORTED, "too many test var pairs");
+        g.pair_a[np] = a;
+        g.pair_b[np] = b;
+        g.hoff[np] = off;
+        off += 4 * g.test[b].ldA;
+        np++;
+      }
+    g.npairs = np;
     g.hstride = off;
+    auto pair_index = [&](int a, int b) { return a * (a + 1) / 2 + b; };
     std::vector<DpgGTile> tiles;
     for (int I = 0; I < g.NBT; I++)
       for (int J = 0; J <= I; J++) {
@@ -556,11 +587,11 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
           if (J >= g.test[v].ntile0 && J < g.test[v].ntile0 + g.test[v].ntiles) b = v;
         }
         DpgGTile t;
-        t.I = I; t.J = J;
-        t.aoff = foff[a] + (I - g.test[a].ntile0) * 8;
-        t.lda = g.test[a].ldA;
-        t.boff = g.hoff[a][b] + (J - g.test[b].ntile0) * 8;
-        t.ldb = g.test[b].ldA;
+        t.I = (int16_t)I; t.J = (int16_t)J;
+        t.aoff = g.test[a].foff + (I - g.test[a].ntile0) * 8;
+        t.lda = (int16_t)g.test[a].ldA;
+        t.boff = g.hoff[pair_index(a, b)] + (J - g.test[b].ntile0) * 8;
+        t.ldb = (int16_t)g.test[b].ldA;
         tiles.push_back(t);
       }
     g.ngt = (int)tiles.size();
@@ -573,14 +604,11 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   }
 
   // ---- B terms, segments, RHS ----------------------------------------------
-  if (D->n_bf + D->n_rhs > DPG_MAX_BF) return fail(DPG_ERR_UNSUPPORTED, "too many bilinear terms");
   if (D->n_rhs > DPG_MAX_RHS) return fail(DPG_ERR_UNSUPPORTED, "too many RHS terms");
-  g.ldT = ld_pad(g.Mp);
-  std::vector<DpgBTerm> terms;
+  std::vector<std::pair<int, DpgBTerm>> terms;  // (segment, term)
   auto test_op_ok = [&](int a, int op, bool side) {
-    const DpgTestVar& tv = g.test[a];
-    if (tv.space == DPG_SPACE_HGRAD) return op == DPG_OP_VALUE || (op >= DPG_OP_DX && op < DPG_OP_DX + d);
-    return (op >= DPG_OP_X && op < DPG_OP_X + d) || op == DPG_OP_DIV || (side && op == DPG_OP_DOT_NORMAL);
+    if (phys_slot(a, op) >= 0) return true;
+    return side && g.test[a].space == DPG_SPACE_HDIV && op == DPG_OP_DOT_NORMAL;
   };
   for (int e = 0; e < D->n_bf; e++) {
     const dpg_bf_term& B = D->bf[e];
@@ -591,6 +619,8 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     if (!test_op_ok(B.test_var, B.test_op, B.boundary)) return fail(DPG_ERR_INVALID_ARGUMENT, "bf test op invalid");
     if (tr.kind != DPG_VAR_FIELD && !B.boundary) return fail(DPG_ERR_INVALID_ARGUMENT, "trace/flux terms must be boundary terms");
     if (B.normal_comp >= d) return fail(DPG_ERR_INVALID_ARGUMENT, "normal component out of range");
+    if ((B.normal_comp >= 0 || B.test_op == DPG_OP_DOT_NORMAL) && !B.boundary)
+      return fail(DPG_ERR_INVALID_ARGUMENT, "normal-dependent terms must be boundary terms");
     int comp = 0;
     if (tr.kind == DPG_VAR_FIELD) {
       if (tr.ncomp > 1) {
@@ -602,14 +632,12 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     for (int sg = 0; sg < nseg; sg++) {
       DpgBTerm t;
       std::memset(&t, 0, sizeof(t));
-      t.trial_var = B.trial_var; t.trial_op = B.trial_op; t.test_var = B.test_var; t.test_op = B.test_op;
+      t.trial_var = B.trial_var; t.test_var = B.test_var; t.test_op = B.test_op;
       t.coef = B.coef; t.slot = B.slot; t.normal_comp = B.normal_comp;
-      t.seg = B.boundary ? 1 + sg : 0;
       t.kind = tr.kind;
-      t.tvar_comp = comp;
       if (tr.kind == DPG_VAR_FIELD) { t.col0 = tr.dev_off + comp * tr.card_comp; t.ncol = tr.card_comp; }
       else { t.col0 = tr.dev_off + sg * tr.per_side; t.ncol = tr.per_side; }
-      terms.push_back(t);
+      terms.push_back({B.boundary ? 1 + sg : 0, t});
     }
   }
   for (int e = 0; e < D->n_rhs; e++) {
@@ -620,85 +648,171 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     DpgBTerm t;
     std::memset(&t, 0, sizeof(t));
     t.trial_var = -1; t.test_var = R.test_var; t.test_op = R.test_op;
-    t.coef = R.coef; t.slot = R.slot; t.normal_comp = -1; t.seg = 0; t.kind = -1;
+    t.coef = R.coef; t.slot = R.slot; t.normal_comp = -1; t.kind = -1;
     t.col0 = g.fcol; t.ncol = 1;
-    terms.push_back(t);
+    terms.push_back({0, t});
   }
-  std::stable_sort(terms.begin(), terms.end(), [](const DpgBTerm& x, const DpgBTerm& y) { return x.seg < y.seg; });
+  std::stable_sort(terms.begin(), terms.end(),
+                   [](const std::pair<int, DpgBTerm>& x, const std::pair<int, DpgBTerm>& y) { return x.first < y.first; });
   if ((int)terms.size() > DPG_MAX_BF) return fail(DPG_ERR_UNSUPPORTED, "too many expanded bilinear terms");
+  g.nbterm = (int)terms.size();
+  for (int i = 0; i < g.nbterm; i++) g.bterm[i] = terms[i].second;
   g.nseg = 1 + g.ns;
+  // all B points: volume (QB) then each side (QS); geometry tables for them
+  g.nbpts = g.QB + g.ns * g.QS;
+  {
+    std::vector<double> xall((size_t)g.nbpts * d), wall(g.nbpts), tall((size_t)g.nbpts * 6, 0.0);
+    for (int q = 0; q < g.QB; q++) {
+      for (int k = 0; k < d; k++) xall[(size_t)q * d + k] = rB.x[(size_t)q * d + k];
+      wall[q] = rB.w[q];
+    }
+    for (int s2 = 0; s2 < g.ns; s2++)
+      for (int q = 0; q < g.QS; q++) {
+        int o = g.QB + s2 * g.QS + q;
+        for (int k = 0; k < d; k++) xall[(size_t)o * d + k] = sidepts[((size_t)s2 * g.QSpad + q) * d + k];
+        for (int k = 0; k < 6; k++) tall[(size_t)o * 6 + k] = sideT[((size_t)s2 * g.QSpad + q) * 6 + k];
+        wall[o] = rS.w[q];
+      }
+    g.dNB = upload(P, dshape(xall, g.nbpts));
+    g.wB = upload(P, wall);
+    g.tangB = upload(P, tall);
+  }
+  // shared-memory budget for the B phase: two record buffers, U, geometry of all
+  // B points, per-point term rows R, coefficients
+  const int budget = 232448 / 8 - 192 - 2 * ((g.ngt * (int)sizeof(DpgGTile) + 7) / 8) - 64 - g.Np - g.Mp - 64;
+  g.max_rec = 0; g.max_chunk = 0; g.max_ustride = 0; g.max_nterm = 0;
   for (int sg = 0; sg < g.nseg; sg++) {
     DpgSeg& S = g.seg[sg];
+    S.side = sg - 1;
     S.npts = sg == 0 ? g.QB : g.QS;
-    S.nops = 0;
+    S.pbase = sg == 0 ? g.QG : g.QG + g.QB + (sg - 1) * g.QS;
+    S.geo0 = sg == 0 ? 0 : g.QB + (sg - 1) * g.QS;
     S.term0 = -1;
     S.nterm = 0;
-    int off = 0;
-    for (int i = 0; i < (int)terms.size(); i++) {
-      DpgBTerm& t = terms[i];
-      if (t.seg != sg) continue;
+    S.nblk = 0;
+    int off = 0, tv = g.featstride;
+    for (int i = 0; i < g.nbterm; i++) {
+      if (terms[i].first != sg) continue;
       if (S.term0 < 0) S.term0 = i;
-      S.nterm++;
-      int k = -1;
-      for (int j = 0; j < S.nops; j++)
-        if (S.ops[j].var == t.test_var && S.ops[j].op == t.test_op) k = j;
-      if (k < 0) {
-        if (S.nops >= DPG_MAX_BOPS) return fail(DPG_ERR_UNSUPPORTED, "too many test ops in a segment");
-        k = S.nops++;
-        S.ops[k].var = t.test_var;
-        S.ops[k].op = t.test_op;
-        S.ops[k].off = off;
-        off += DPG_CHUNK * g.test[t.test_var].ldA;
+      int lt = S.nterm++;
+      if (lt >= DPG_MAX_BF / 4) return fail(DPG_ERR_UNSUPPORTED, "too many terms in one segment");
+      const DpgBTerm& t = g.bterm[i];
+      S.tvoff[lt] = tv;
+      tv += t.ncol;
+      for (int J = t.col0 / 8; J <= (t.col0 + t.ncol - 1) / 8; J++) {
+        int k = -1;
+        for (int kk = 0; kk < S.nblk; kk++)
+          if (S.blk[kk].var == t.test_var && S.blk[kk].J == J) k = kk;
+        if (k < 0) {
+          if (S.nblk >= DPG_MAX_BLK) return fail(DPG_ERR_UNSUPPORTED, "too many active B blocks in a segment");
+          k = S.nblk++;
+          S.blk[k].var = t.test_var;
+          S.blk[k].J = J;
+          S.blk[k].off = off;
+          S.blk[k].nt = 0;
+          off += 4 * DPG_ULD;
+        }
+        if (S.blk[k].nt >= DPG_MAX_BT) return fail(DPG_ERR_UNSUPPORTED, "too many terms feeding one B block");
+        S.blk[k].terms[S.blk[k].nt++] = lt;
       }
-      t.bop = k;
     }
     if (S.term0 < 0) S.term0 = 0;
-    S.opstride = off;
+    S.ustride = off;
+    S.rec_len = (tv + 1) & ~1;
+    g.max_rec = std::max(g.max_rec, S.rec_len);
+    g.max_ustride = std::max(g.max_ustride, S.ustride);
+    g.max_nterm = std::max(g.max_nterm, S.nterm);
   }
-  g.nbterm = (int)terms.size();
-  for (int i = 0; i < g.nbterm; i++) g.bterm[i] = terms[i];
-
-  // ---- geometry uploads ------------------------------------------------------
-  g.dNG = upload(P, dNG);
-  g.dNB = upload(P, dNB);
-  g.dNS = upload(P, dNS);
-  g.wG = upload(P, rG.w);
-  g.wB = upload(P, rB.w);
-  g.wS = upload(P, rS.w);
-  g.sideT = upload(P, sideT);
+  // chunk size: all points of a side in one chunk when it fits; the volume in equal chunks
+  {
+    auto fits = [&](int ch) {
+      int need = 2 * ch * g.max_rec + ch * g.max_ustride + g.nbpts * 24 + ch * g.max_nterm * 4 +
+                 g.nslots * g.Ptot + 64;
+      return need <= budget;
+    };
+    int ch = std::min(DPG_MAX_CHB, std::max(g.QS, 1));
+    while (ch > 1 && !fits(ch)) ch--;
+    if (!fits(ch)) return fail(DPG_ERR_UNSUPPORTED, "B-phase staging does not fit in shared memory");
+    for (int sg = 0; sg < g.nseg; sg++) {
+      DpgSeg& S = g.seg[sg];
+      int nch = (S.npts + ch - 1) / ch;
+      S.nchunk = nch;
+      S.chunk = (S.npts + nch - 1) / nch;  // balanced chunks
+      g.max_chunk = std::max(g.max_chunk, S.chunk);
+    }
+  }
+  // per-segment point records: reference slots of every test var, then each term's trial values
+  for (int sg = 0; sg < g.nseg; sg++) {
+    DpgSeg& S = g.seg[sg];
+    const int npad = S.nchunk * S.chunk;
+    std::vector<double> xs((size_t)npad * d, 0.0);
+    for (int q = 0; q < npad; q++) {
+      int src = q < S.npts ? q : 0;
+      for (int k = 0; k < d; k++)
+        xs[(size_t)q * d + k] = (sg == 0) ? rB.x[(size_t)src * d + k]
+                                          : sidepts[((size_t)(sg - 1) * g.QSpad + src) * d + k];
+    }
+    std::vector<double> slots = fref_table(xs.data(), npad);
+    std::vector<double> rec((size_t)npad * S.rec_len, 0.0);
+    for (int q = 0; q < npad; q++) {
+      std::copy(slots.begin() + (size_t)q * g.featstride, slots.begin() + (size_t)(q + 1) * g.featstride,
+                rec.begin() + (size_t)q * S.rec_len);
+      if (q >= S.npts) continue;
+      for (int lt = 0; lt < S.nterm; lt++) {
+        const DpgBTerm& t = g.bterm[S.term0 + lt];
+        double* dst = &rec[(size_t)q * S.rec_len + S.tvoff[lt]];
+        if (t.kind < 0) { dst[0] = 1.0; continue; }
+        const DpgTrialVar& tr = g.trial[t.trial_var];
+        for (int m = 0; m < t.ncol; m++) {
+          if (t.kind == DPG_VAR_FIELD)
+            dst[m] = (sg == 0) ? host_tabB[t.trial_var][(size_t)q * tr.card_comp + m]
+                               : host_tabS[t.trial_var][((size_t)(sg - 1) * g.QSpad + q) * tr.card_comp + m];
+          else
+            dst[m] = host_tabS[t.trial_var][(size_t)q * tr.per_side + m];
+        }
+      }
+    }
+    S.rec = upload(P, rec);
+  }
 
   // ---- shared memory layout (doubles) ----------------------------------------
   {
-    int geo = DPG_CHUNK * 32;
-    int cm = DPG_CHUNK * g.Ftot * g.Ftot + DPG_CHUNK * DPG_MAX_IPROWS * g.Ftot;
-    int gphase = geo + cm + DPG_CHUNK * g.featstride + DPG_CHUNK * g.hstride;
-    g.sm_geo = 0;
-    g.sm_cmat = geo;
-    g.sm_feat = geo + cm;
-    g.sm_h = g.sm_feat + DPG_CHUNK * g.featstride;
-    g.sm_gt = 0;
-    int gt = g.ngt * 64;
-    g.sm_linv = gt;
-    g.sm_scale = g.sm_linv + g.NBT * 64;
-    int geo2 = g.sm_scale + g.Np;
-    // B phase: geometry of the chunk, staged ops, staged trial values
-    int maxops = 0, maxterm = 0;
-    for (int sg = 0; sg < g.nseg; sg++) {
-      maxops = std::max(maxops, g.seg[sg].opstride);
-      maxterm = std::max(maxterm, g.seg[sg].nterm);
-    }
-    g.sm_misc = geo2;                       // chunk geometry for the B phase (DPG_CHUNK * 32)
-    g.sm_bops = g.sm_misc + DPG_CHUNK * 32;
-    g.sm_bval = g.sm_bops + maxops;
-    int bphase = g.sm_bval + maxterm * DPG_CHUNK * g.ldT;
+    auto al = [](int x) { return (x + 15) & ~15; };  // 128-byte aligned regions
+    int o = 0;
+    // Gram phase
+    g.g_fref0 = o; o += al(DPG_CHG * g.featstride);
+    g.g_fref1 = o; o += al(DPG_CHG * g.featstride);
+    g.g_h = o; o += al(DPG_CHG * g.hstride);
+    g.g_geo = o; o += al(g.QGpad * 24);
+    g.g_D = o; o += al(g.QGpad * g.npairs * 16);
+    int gphase = o;
+    // factor
+    o = 0;
+    g.sm_gt = o; o += al(g.ngt * 64);
+    g.sm_linv = o; o += al(g.NBT * 64);
+    g.sm_scale = o; o += al(g.Np);
+    int fphase = o;
+    // B phase (runs first; whole body available)
+    o = 0;
+    g.b_rec0 = o; o += al(g.max_chunk * g.max_rec);
+    g.b_rec1 = o; o += al(g.max_chunk * g.max_rec);
+    g.b_u = o; o += al(g.max_chunk * g.max_ustride);
+    g.b_geo = o; o += al(g.nbpts * 24);
+    g.b_R = o; o += al(g.max_chunk * g.max_nterm * 4);
+    int bphase = o;
     g.sm_w = 0;
     int wsz = g.MBT * g.NBT * 64;
     g.sm_k = 0;
     int ksz = g.MBT * (g.MBT + 1) / 2 * 64;
-    int total = std::max(std::max(gphase, bphase), std::max(wsz, ksz));
-    g.sm_total = total + 64;  // + cell nodes / flags
+    int body = std::max(std::max(gphase, bphase), std::max(std::max(wsz, ksz), fphase));
+    g.sm_coef = al(body);
+    g.sm_tiles = g.sm_coef + al(std::max(1, g.nslots * g.Ptot));
+    g.sm_nodes = g.sm_tiles + al((g.ngt * (int)sizeof(DpgGTile) + 7) / 8);
+    g.sm_invd = g.sm_nodes + 192;
+    g.sm_total = g.sm_invd + al(std::max(g.Np, g.Mp));
     if ((size_t)g.sm_total * 8 > 232448)
       return fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
+    g.scratch_per_cta = (size_t)g.MBT * g.NBT * 64;
   }
   // info
   dpg_plan_info& I = P->info;
@@ -706,7 +820,6 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   I.space_dim = d; I.n_vertices = T.nv; I.n_sides = T.ns;
   I.Q_G = g.QG; I.Q_B = g.QB; I.Q_side = g.QS; I.n_points_total = g.Ptot;
   I.n_slots = g.nslots; I.precision = D->precision;
-  // device copy of the plan
   void* p = nullptr;
   if (cudaMalloc(&p, sizeof(DpgPlanDev)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc plan");
   cudaMemcpy(p, &g, sizeof(DpgPlanDev), cudaMemcpyHostToDevice);
@@ -727,6 +840,7 @@ int dpg_make_solve_plan(int N, int M, DpgPlanDev* out) {
   DpgPlanDev& g = *out;
   std::memset(&g, 0, sizeof(g));
   auto pad8 = [](int n) { return (n + 7) & ~7; };
+  auto al = [](int x) { return (x + 15) & ~15; };
   g.d = 2; g.nv = 0; g.ns = 0;
   g.N = N; g.M = M; g.nf = M; g.nt = 0;
   g.Np = pad8(N); g.NBT = g.Np / 8;
@@ -739,12 +853,17 @@ int dpg_make_solve_plan(int N, int M, DpgPlanDev* out) {
   g.trial[0].kind = DPG_VAR_FIELD; g.trial[0].ncomp = 1; g.trial[0].card_comp = M;
   g.ngt = g.NBT * (g.NBT + 1) / 2;
   g.sm_gt = 0;
-  g.sm_linv = g.ngt * 64;
-  g.sm_scale = g.sm_linv + g.NBT * 64;
-  int a = g.sm_scale + g.Np;
+  g.sm_linv = al(g.ngt * 64);
+  g.sm_scale = g.sm_linv + al(g.NBT * 64);
+  int a = g.sm_scale + al(g.Np);
   int w = g.MBT * g.NBT * 64, k = g.MBT * (g.MBT + 1) / 2 * 64;
   g.sm_w = 0; g.sm_k = 0;
-  g.sm_total = std::max(a, std::max(w, k)) + 64;
+  g.sm_coef = al(std::max(a, std::max(w, k)));
+  g.sm_tiles = g.sm_coef;
+  g.sm_nodes = g.sm_tiles;
+  g.scratch_per_cta = 0;
+  g.sm_invd = g.sm_nodes + 192;
+  g.sm_total = g.sm_invd + al(std::max(g.Np, g.Mp));
   return DPG_OK;
 }
 

@@ -32,6 +32,8 @@ struct DpgLaunch {
   const double* Gin;
   const double* Bin;
   const double* Fin;
+  // B tiles between the B phase and the triangular solve: scratch_per_cta doubles per CTA
+  double* scratch;
 };
 
 int dpg_configure_kernels(const DpgPlanDev* plan);

@@ -1,14 +1,20 @@
 // dpg_kernel.cu — fused FP64 per-cell DPG assembly for sm_100a.
 //
-// One CTA (16 warps) assembles one cell end to end:
-//   1. Gram matrix G (BasisCache + IP::computeInnerProductMatrix, IP.cpp:215-292):
-//      physical test features are staged in shared memory four quadrature
-//      points at a time; every warp owns a contiguous run of lower 8x8 tiles of
-//      G and accumulates them in registers with mma.m8n8k4.f64 (DMMA).
-//   2. Equilibrated Cholesky of G (BF.cpp:944-982: DPOEQU scaling, DPOTRF('L'),
+// Persistent CTAs (16 warps, one per SM) walk the cells.  Per cell:
+//   1. B and F (TBF::stiffnessMatrix, BF.cpp:575-656; RHS.cpp:68-82): per
+//      quadrature segment (volume, each side) the per-point records — reference
+//      slots of the test bases plus each term's trial values — arrive by bulk
+//      (TMA) copy, double buffered.  The Piola maps, normals, parities and
+//      coefficients of every term collapse into one 4-vector per point (R), the
+//      coupling U = R * trial values is formed per active (test var, column tile)
+//      block, and warp J accumulates B[:, J] in registers with mma.m8n8k4.f64
+//      (DMMA).  The tiles wait in a per-CTA scratch slot (L2-resident).
+//   2. Gram matrix G (IP::computeInnerProductMatrix, IP.cpp:215-292): the same
+//      slot form; per point and test-var pair a 4x4 coupling D = T_a^T C T_b
+//      (C: graph-norm coefficients, T: Piola maps) is built once, h = D * slots
+//      per chunk, and every warp accumulates a run of lower 8x8 tiles of G.
+//   3. Equilibrated Cholesky of G (BF.cpp:944-982: DPOEQU scaling, DPOTRF('L'),
 //      unscaling), blocked right-looking on tiles held in shared memory.
-//   3. B and F (TBF::stiffnessMatrix, BF.cpp:575-656; RHS.cpp:68-82): warp J owns
-//      trial column tile J and accumulates all of B[:, J] in registers.
 //   4. W = L^-1 [B | F] in registers (BF.cpp:987-988, 1013-1014): each warp runs
 //      a blocked forward substitution on its own column tile; diagonal blocks use
 //      precomputed inverses so every step is a DMMA.
@@ -30,6 +36,9 @@
 namespace {
 
 constexpr int NT = DPG_NTHREADS;
+constexpr int MBAR_SPIN_LIMIT = 1 << 22;
+constexpr int ERR_TIMEOUT_FLAG = 0x7fff0000;
+constexpr int GEO = 24;  // doubles per point geometry record: J(9) Ji(9) det w*|J| n(3) pad
 
 __device__ __forceinline__ void dmma(double2& c, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -37,18 +46,43 @@ __device__ __forceinline__ void dmma(double2& c, double a, double b) {
                : "d"(a), "d"(b));
 }
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+
+// Global -> shared bulk copy completing on an mbarrier (16-byte aligned, bytes % 16 == 0).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(b))
+               : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false if the limit was reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  for (int it = 0; it < MBAR_SPIN_LIMIT; it++) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // AK layout index of element (r, c) of an 8x8 tile
 __device__ __forceinline__ int ak(int r, int c) { return ((c >> 2) * 8 + r) * 4 + (c & 3); }
 
 // Offset of the C-fragment pair (g, 2t..2t+1) in AK layout
 __device__ __forceinline__ int ak_cfrag(int g, int t) { return ((t >> 1) * 8 + g) * 4 + (t & 1) * 2; }
-
-__device__ __forceinline__ int tri_row(int tau) {
-  int I = (int)((sqrt(8.0 * tau + 1.0) - 1.0) * 0.5);
-  while ((I + 1) * (I + 2) / 2 <= tau) I++;
-  while (I * (I + 1) / 2 > tau) I--;
-  return I;
-}
 
 // Convert a C-fragment (rows g, cols 2t, 2t+1) into the two B-fragments of the
 // same 8x8 matrix used as the k x n operand: B_h[t][g] = X[4h + t][g].
@@ -64,71 +98,138 @@ __device__ __forceinline__ void cfrag_to_bfrag(const double2 c, int lane, double
   b1 = (g & 1) ? y1 : x1;
 }
 
-struct Geo {
-  double J[9], Ji[9], det;
-};
-
-// Jacobian, inverse and determinant from the vertex-shape derivatives at a point.
-__device__ __forceinline__ void geometry(int d, int nv, const double* __restrict__ X, const double* __restrict__ dN,
-                                         Geo& G) {
+// Geometry record of one point: Jacobian, inverse, determinant, weighted
+// measure (w*detJ, or w*|side Jacobian| when tang != nullptr) and, on a side,
+// the outward unit normal.  All vertex-shape derivatives are loaded up front.
+__device__ __forceinline__ void point_geometry(int d, int nv, const double* __restrict__ X,
+                                               const double* __restrict__ dN, double w,
+                                               const double* __restrict__ tang, double* gq) {
+  double dn[24];
 #pragma unroll
-  for (int i = 0; i < 9; i++) G.J[i] = 0.0;
-  for (int a = 0; a < nv; a++)
-    for (int i = 0; i < d; i++) {
-      double xa = X[a * d + i];
-      for (int j = 0; j < d; j++) G.J[i * 3 + j] += xa * dN[a * d + j];
+  for (int i = 0; i < 24; i++) dn[i] = (i < nv * d) ? __ldg(dN + i) : 0.0;
+  double tg[6];
+  if (tang) {
+#pragma unroll
+    for (int i = 0; i < 6; i++) tg[i] = __ldg(tang + i);
+  }
+  double J[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) J[i] = 0.0;
+  if (d == 3) {
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      if (a < nv) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          double xa = X[a * 3 + i];
+#pragma unroll
+          for (int j = 0; j < 3; j++) J[i * 3 + j] += xa * dn[a * 3 + j];
+        }
+      }
     }
-  if (d == 2) {
-    G.det = G.J[0] * G.J[4] - G.J[1] * G.J[3];
-    double id = 1.0 / G.det;
-    G.Ji[0] = G.J[4] * id; G.Ji[1] = -G.J[1] * id; G.Ji[2] = 0;
-    G.Ji[3] = -G.J[3] * id; G.Ji[4] = G.J[0] * id; G.Ji[5] = 0;
-    G.Ji[6] = 0; G.Ji[7] = 0; G.Ji[8] = 1;
   } else {
-    const double* A = G.J;
-    double c00 = A[4] * A[8] - A[5] * A[7];
-    double c01 = A[5] * A[6] - A[3] * A[8];
-    double c02 = A[3] * A[7] - A[4] * A[6];
-    G.det = A[0] * c00 + A[1] * c01 + A[2] * c02;
-    double id = 1.0 / G.det;
-    G.Ji[0] = c00 * id;
-    G.Ji[3] = c01 * id;
-    G.Ji[6] = c02 * id;
-    G.Ji[1] = (A[2] * A[7] - A[1] * A[8]) * id;
-    G.Ji[4] = (A[0] * A[8] - A[2] * A[6]) * id;
-    G.Ji[7] = (A[1] * A[6] - A[0] * A[7]) * id;
-    G.Ji[2] = (A[1] * A[5] - A[2] * A[4]) * id;
-    G.Ji[5] = (A[2] * A[3] - A[0] * A[5]) * id;
-    G.Ji[8] = (A[0] * A[4] - A[1] * A[3]) * id;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      if (a < nv) {
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          double xa = X[a * 2 + i];
+#pragma unroll
+          for (int j = 0; j < 2; j++) J[i * 3 + j] += xa * dn[a * 2 + j];
+        }
+      }
+    }
+  }
+  double Ji[9], det;
+  if (d == 2) {
+    det = J[0] * J[4] - J[1] * J[3];
+    double id = 1.0 / det;
+    Ji[0] = J[4] * id; Ji[1] = -J[1] * id; Ji[2] = 0;
+    Ji[3] = -J[3] * id; Ji[4] = J[0] * id; Ji[5] = 0;
+    Ji[6] = 0; Ji[7] = 0; Ji[8] = 1;
+  } else {
+    double c00 = J[4] * J[8] - J[5] * J[7];
+    double c01 = J[5] * J[6] - J[3] * J[8];
+    double c02 = J[3] * J[7] - J[4] * J[6];
+    det = J[0] * c00 + J[1] * c01 + J[2] * c02;
+    double id = 1.0 / det;
+    Ji[0] = c00 * id;
+    Ji[3] = c01 * id;
+    Ji[6] = c02 * id;
+    Ji[1] = (J[2] * J[7] - J[1] * J[8]) * id;
+    Ji[4] = (J[0] * J[8] - J[2] * J[6]) * id;
+    Ji[7] = (J[1] * J[6] - J[0] * J[7]) * id;
+    Ji[2] = (J[1] * J[5] - J[2] * J[4]) * id;
+    Ji[5] = (J[2] * J[3] - J[0] * J[5]) * id;
+    Ji[8] = (J[0] * J[4] - J[1] * J[3]) * id;
+  }
+#pragma unroll
+  for (int i = 0; i < 9; i++) { gq[i] = J[i]; gq[9 + i] = Ji[i]; }
+  gq[18] = det;
+  gq[20] = gq[21] = gq[22] = 0.0;
+  if (!tang) {
+    gq[19] = w * det;
+    return;
+  }
+  double T0[3] = {0, 0, 0}, T1[3] = {0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      T0[i] += J[i * 3 + j] * tg[j];
+      T1[i] += J[i * 3 + j] * tg[3 + j];
+    }
+  double meas;
+  if (d == 2) {
+    meas = sqrt(T0[0] * T0[0] + T0[1] * T0[1]);
+    gq[20] = T0[1] / meas;
+    gq[21] = -T0[0] / meas;
+  } else {
+    double c0 = T0[1] * T1[2] - T0[2] * T1[1];
+    double c1 = T0[2] * T1[0] - T0[0] * T1[2];
+    double c2 = T0[0] * T1[1] - T0[1] * T1[0];
+    meas = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    gq[20] = c0 / meas; gq[21] = c1 / meas; gq[22] = c2 / meas;
+  }
+  gq[19] = w * meas;
+}
+
+// Row `m` of the slot transform T of a test var at a point: physical value of
+// the operator in physical slot m = sum_k T[m][k] * reference slot k.
+//   HGRAD slots (value, d/dx_0..): T[0][0] = 1, T[1+c][1+j] = Ji[j][c]
+//   HDIV  slots (v_0.., div):      T[c][j] = J[c][j]/det, T[d][d] = 1/det
+__device__ __forceinline__ void trow_slot(int space, int d, int m, const double* gq, double* r) {
+  r[0] = r[1] = r[2] = r[3] = 0.0;
+  if (space == DPG_SPACE_HGRAD) {
+    if (m == 0) r[0] = 1.0;
+    else if (m <= d) {
+      int c = m - 1;
+      for (int j = 0; j < d; j++) r[1 + j] = gq[9 + j * 3 + c];
+    }
+  } else {
+    double id = 1.0 / gq[18];
+    if (m < d) {
+      for (int j = 0; j < d; j++) r[j] = gq[m * 3 + j] * id;
+    } else if (m == d) {
+      r[d] = id;
+    }
   }
 }
 
-// Physical value of a test operator from the reference record of one dof.
-// geo: [J(9) Ji(9) det wdet meas n(3)]
-__device__ __forceinline__ double test_op(int space, int d, int op, const double* __restrict__ ref,
-                                          const double* __restrict__ geo) {
+// Row of T for a physical operator (incl. tau . n on a side; normal at gq[20..22]).
+__device__ __forceinline__ void trow_op(int space, int d, int op, const double* gq, double* r) {
   if (space == DPG_SPACE_HGRAD) {
-    if (op == DPG_OP_VALUE) return ref[0];
-    int c = op - DPG_OP_DX;  // (J^-T grad)_c = sum_j Ji[j][c] grad_j
-    double s = 0.0;
-    for (int j = 0; j < d; j++) s += geo[9 + j * 3 + c] * ref[1 + j];
-    return s;
+    trow_slot(space, d, op == DPG_OP_VALUE ? 0 : 1 + (op - DPG_OP_DX), gq, r);
+    return;
   }
-  double idet = 1.0 / geo[18];
-  if (op == DPG_OP_DIV) return ref[d] * idet;
   if (op == DPG_OP_DOT_NORMAL) {
-    double s = 0.0;
-    for (int c = 0; c < d; c++) {
-      double v = 0.0;
-      for (int j = 0; j < d; j++) v += geo[c * 3 + j] * ref[j];
-      s += v * geo[21 + c];
-    }
-    return s * idet;
+    double id = 1.0 / gq[18];
+    r[0] = r[1] = r[2] = r[3] = 0.0;
+    for (int c = 0; c < d; c++)
+      for (int j = 0; j < d; j++) r[j] += gq[20 + c] * gq[c * 3 + j] * id;
+    return;
   }
-  int c = op - DPG_OP_X;
-  double v = 0.0;
-  for (int j = 0; j < d; j++) v += geo[c * 3 + j] * ref[j];
-  return v * idet;
+  trow_slot(space, d, op == DPG_OP_DIV ? d : op - DPG_OP_X, gq, r);
 }
 
 // Element (r, c) of the symmetric matrix stored as lower AK tiles at base.
@@ -138,10 +239,23 @@ __device__ __forceinline__ double sym_get(const double* base, int r, int c) {
   return base[(I * (I + 1) / 2 + J) * 64 + ak(r & 7, c & 7)];
 }
 
+struct Ctx {
+  double* sm;
+  int* flag;        // [0] Gram pivot, [1] condensation pivot, [2] staging timeout
+  uint64_t* mbar;   // [0,1] Gram slots, [2,3] B records
+  const int* tri;   // lower tile index -> (I | J << 8)
+  const DpgGTile* tiles;
+  const double* nodes;
+  const double* coef;  // this cell's coefficients [nslots][Ptot]
+  double* invd;        // inverse pivots of the current factorisation
+  uint32_t* phase;     // mbarrier use counters [4]
+};
+
 // Blocked right-looking Cholesky of the leading nsteps tiles of a tile-lower
-// matrix with nb tiles in shared memory.  Records the first failing global
-// pivot (1-based) into *flag with sign `sgn` if *flag is still 0.
-__device__ void tile_cholesky(double* __restrict__ T, int nb, int nsteps, int* flag, int sgn) {
+// matrix with nb tiles in shared memory.  invd[8k + j] receives 1 / L_jj.
+// Records the first failing global pivot (1-based) into *flag with sign `sgn`.
+__device__ __noinline__ void tile_cholesky(double* __restrict__ T, int nb, int nsteps, int* flag, int sgn,
+                                           const int* tri, double* invd) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   for (int k = 0; k < nsteps; k++) {
@@ -157,9 +271,8 @@ __device__ void tile_cholesky(double* __restrict__ T, int nb, int nsteps, int* f
       for (int j = 0; j < 8; j++) {
         double piv = __shfl_sync(0xffffffffu, row[j], j);
         if (!(piv > 0.0) && !failed) { failed = true; fail_j = j; }
-        double dj = sqrt(piv);
-        double inv = 1.0 / dj;
-        if (r == j) row[j] = dj;
+        double inv = rsqrt(piv);
+        if (r == j) { row[j] = piv * inv; if (lane < 8) invd[k * 8 + j] = inv; }
         else if (r > j) row[j] *= inv;
 #pragma unroll
         for (int c = j + 1; c < 8; c++) {
@@ -175,7 +288,8 @@ __device__ void tile_cholesky(double* __restrict__ T, int nb, int nsteps, int* f
     }
     __syncthreads();
     // panel: L_ik = A_ik L_kk^-T, one row per thread
-    int nrows = (nb - 1 - k) * 8;
+    const int nrows = (nb - 1 - k) * 8;
+    const double* iv = invd + k * 8;
     for (int w = tid; w < nrows; w += NT) {
       int i = k + 1 + (w >> 3), r = w & 7;
       double* Tik = T + (i * (i + 1) / 2 + k) * 64;
@@ -187,18 +301,18 @@ __device__ void tile_cholesky(double* __restrict__ T, int nb, int nsteps, int* f
         double v = x[c];
 #pragma unroll
         for (int m = 0; m < c; m++) v -= x[m] * Tkk[ak(c, m)];
-        x[c] = v / Tkk[ak(c, c)];
+        x[c] = v * iv[c];
       }
 #pragma unroll
       for (int c = 0; c < 8; c++) Tik[ak(r, c)] = x[c];
     }
     __syncthreads();
     // trailing update: A_ij -= L_ik L_jk^T for k < j <= i < nb
-    int m = nb - 1 - k;
-    int ntr = m * (m + 1) / 2;
+    const int m = nb - 1 - k;
+    const int ntr = m * (m + 1) / 2;
     for (int u = warp; u < ntr; u += DPG_NWARPS) {
-      int ii = tri_row(u), jj = u - ii * (ii + 1) / 2;
-      int i = k + 1 + ii, j = k + 1 + jj;
+      int ij = tri[u];
+      int i = k + 1 + (ij & 255), j = k + 1 + (ij >> 8);
       double* Tij = T + (i * (i + 1) / 2 + j) * 64;
       const double* Lik = T + (i * (i + 1) / 2 + k) * 64;
       const double* Ljk = T + (j * (j + 1) / 2 + k) * 64;
@@ -211,220 +325,377 @@ __device__ void tile_cholesky(double* __restrict__ T, int nb, int nsteps, int* f
   }
 }
 
+// ---------------------------------------------------------------------------
+// Phase 1: B and F -> per-CTA scratch (or the B/F outputs in parts mode)
+// ---------------------------------------------------------------------------
 template <int NBTM>
-__global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
-  extern __shared__ __align__(16) double sm[];
+__device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int cell = blockIdx.x;
   const int d = P.d, nv = P.nv;
-  double* nodes_s = sm + P.sm_total - 64;
-  int* flag_s = reinterpret_cast<int*>(sm + P.sm_total - 8);
-  if (!L.solve_only && tid < nv * d) nodes_s[tid] = L.nodes[(size_t)cell * nv * d + tid];
-  if (tid == 0) { flag_s[0] = 0; flag_s[1] = 0; }
-  const double* coef_c = L.coeff ? L.coeff + (size_t)cell * P.nslots * P.Ptot : nullptr;
-  const int8_t* par_c = L.solve_only ? nullptr : L.parity + (size_t)cell * P.ns;
-  __syncthreads();
-
-  double* GT = sm + P.sm_gt;  // lower tiles of G, AK layout
-
-  // ======================= 1. Gram matrix ===================================
-  if (L.solve_only) {
-    const double* Gc = L.Gin + (size_t)cell * P.N * P.N;
-    for (int e = tid; e < P.ngt * 64; e += NT) {
-      int tau = e >> 6, idx = e & 63;
-      int I = tri_row(tau), J = tau - I * (I + 1) / 2;
-      int r = (idx >> 2) & 7, c = (idx >> 5) * 4 + (idx & 3);
-      int gr = I * 8 + r, gc = J * 8 + c;
-      double v = 0.0;
-      if (gr < P.N && gc < P.N) v = Gc[(size_t)gr * P.N + gc];
-      else if (gr == gc) v = 1.0;
-      GT[e] = v;
-    }
-    __syncthreads();
-  } else {
-    const int per = (P.ngt + DPG_NWARPS - 1) / DPG_NWARPS;
-    const int tau0 = warp * per;
-    const int ntw = max(0, min(per, P.ngt - tau0));
-    double2 acc[DPG_MAX_GT];
-#pragma unroll
-    for (int u = 0; u < DPG_MAX_GT; u++) acc[u] = make_double2(0.0, 0.0);
-    double* geo = sm + P.sm_geo;
-    double* avec = sm + P.sm_cmat + DPG_CHUNK * P.Ftot * P.Ftot;  // [q][row][F]
-    double* cm = sm + P.sm_cmat;                                   // [q][F][F]
-    double* feat = sm + P.sm_feat;
-    double* hb = sm + P.sm_h;
-    const int F = P.Ftot;
-    for (int q0 = 0; q0 < P.QG; q0 += DPG_CHUNK) {
-      const int np = min(DPG_CHUNK, P.QG - q0);
-      if (tid < DPG_CHUNK) {
-        double* gq = geo + tid * 32;
-        if (tid < np) {
-          Geo G;
-          geometry(d, nv, nodes_s, P.dNG + (size_t)(q0 + tid) * nv * d, G);
-#pragma unroll
-          for (int i = 0; i < 9; i++) { gq[i] = G.J[i]; gq[9 + i] = G.Ji[i]; }
-          gq[18] = G.det;
-          gq[19] = P.wG[q0 + tid] * G.det;
-        } else {
-#pragma unroll
-          for (int i = 0; i < 9; i++) { gq[i] = (i % 4 == 0) ? 1.0 : 0.0; gq[9 + i] = gq[i]; }
-          gq[18] = 1.0;
-          gq[19] = 0.0;
-        }
-      }
-      for (int i = tid; i < DPG_CHUNK * DPG_MAX_IPROWS * F; i += NT) avec[i] = 0.0;
-      __syncthreads();
-      if (tid < DPG_CHUNK) {
-        const int q = tid;
-        for (int e = 0; e < P.nipent; e++) {
-          const DpgIPEnt& E = P.ipent[e];
-          double v = E.coef;
-          if (E.slot >= 0) v *= (q < np) ? coef_c[(size_t)E.slot * P.Ptot + q0 + q] : 0.0;
-          avec[(q * DPG_MAX_IPROWS + E.row) * F + E.gfeat] += v;
-        }
-      }
-      // physical features [q][var][4][ldA]
-      for (int q = 0; q < DPG_CHUNK; q++) {
-        const double* gq = geo + q * 32;
-        int foff = 0;
-        for (int a = 0; a < P.ntest; a++) {
-          const DpgTestVar& V = P.test[a];
-          const int n = 4 * V.ldA;
-          double* dst = feat + q * P.featstride + foff;
-          for (int i = tid; i < n; i += NT) {
-            int k = i / V.ldA, row = i - k * V.ldA;
-            double v = 0.0;
-            if (q < np && k < V.nfeat && row < V.card)
-              v = test_op(V.space, d, V.feat_op[k], V.tabG + ((size_t)(q0 + q) * V.card + row) * V.nref, gq);
-            dst[i] = v;
-          }
-          foff += n;
-        }
-      }
-      __syncthreads();
-      // coefficient matrix C_q = wdet * sum_r a_r a_r^T
-      for (int i = tid; i < DPG_CHUNK * F * F; i += NT) {
-        int q = i / (F * F), rem = i - q * F * F, f1 = rem / F, f2 = rem - f1 * F;
-        double s = 0.0;
-        const double* aq = avec + q * DPG_MAX_IPROWS * F;
-        for (int r = 0; r < P.niprows; r++) s += aq[r * F + f1] * aq[r * F + f2];
-        cm[i] = s * geo[q * 32 + 19];
-      }
-      __syncthreads();
-      // h_{b->a}[q][k][j] = sum_l C[4a+k][4b+l] f_b[q][l][j]
-      for (int q = 0; q < DPG_CHUNK; q++) {
-        const double* Cq = cm + q * F * F;
-        for (int a = 0; a < P.ntest; a++) {
-          int foff_b = 0;
-          for (int b = 0; b <= a; b++) {
-            const DpgTestVar& Vb = P.test[b];
-            const int n = 4 * Vb.ldA;
-            const double* fb = feat + q * P.featstride + foff_b;
-            double* dst = hb + q * P.hstride + P.hoff[a][b];
-            for (int i = tid; i < n; i += NT) {
-              int k = i / Vb.ldA, j = i - k * Vb.ldA;
-              const double* crow = Cq + (4 * a + k) * F + 4 * b;
-              dst[i] = crow[0] * fb[j] + crow[1] * fb[Vb.ldA + j] + crow[2] * fb[2 * Vb.ldA + j] +
-                       crow[3] * fb[3 * Vb.ldA + j];
-            }
-            foff_b += n;
-          }
-        }
-      }
-      __syncthreads();
-      // DMMA accumulation of the owned tiles
-      for (int q = 0; q < np; q++) {
-        const double* fq = feat + q * P.featstride;
-        const double* hq = hb + q * P.hstride;
-        int lastI = -1;
-        double afr = 0.0;
-#pragma unroll
-        for (int u = 0; u < DPG_MAX_GT; u++) {
-          if (u < ntw) {
-            const DpgGTile T = P.gtiles[tau0 + u];
-            if (T.I != lastI) { afr = fq[T.aoff + t * T.lda + g]; lastI = T.I; }
-            double bfr = hq[T.boff + t * T.ldb + g];
-            dmma(acc[u], afr, bfr);
-          }
-        }
-      }
-      __syncthreads();
-    }
-    // accumulators -> tile-lower shared storage (overlaps the staging area)
-#pragma unroll
-    for (int u = 0; u < DPG_MAX_GT; u++)
-      if (u < ntw) *reinterpret_cast<double2*>(GT + (tau0 + u) * 64 + ak_cfrag(g, t)) = acc[u];
-    __syncthreads();
-    // padded rows decouple: unit diagonal
-    for (int r = tid; r < P.Np; r += NT)
-      if (P.dev2user_test[r] < 0) GT[((r >> 3) * ((r >> 3) + 1) / 2 + (r >> 3)) * 64 + ak(r & 7, r & 7)] = 1.0;
-    __syncthreads();
-    if (L.parts && L.G) {
-      double* Gc = L.G + (size_t)cell * P.N * P.N;
-      for (int e = tid; e < P.Np * P.Np; e += NT) {
-        int r = e / P.Np, c = e - r * P.Np;
-        int ur = P.dev2user_test[r], uc = P.dev2user_test[c];
-        if (ur >= 0 && uc >= 0) Gc[(size_t)ur * P.N + uc] = sym_get(GT, r, c);
-      }
-    }
+  double* sm = X.sm;
+  double* geo = sm + P.b_geo;
+  double* U = sm + P.b_u;
+  double* R = sm + P.b_R;
+  const int8_t* par_c = L.parity + (size_t)cell * P.ns;
+  // prologue: first chunk's records in flight while the geometry is computed
+  int first_seg = 0;
+  while (first_seg < P.nseg && P.seg[first_seg].nterm == 0) first_seg++;
+  if (tid == 0 && first_seg < P.nseg) {
+    const DpgSeg& S = P.seg[first_seg];
+    const uint32_t bytes = (uint32_t)(S.chunk * S.rec_len * sizeof(double));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&X.mbar[2], bytes);
+    bulk_g2s(sm + P.b_rec0, S.rec, bytes, &X.mbar[2]);
   }
-
-  // ======================= 2. equilibrated Cholesky ==========================
-  double* scale = sm + P.sm_scale;
-  double* LINV = sm + P.sm_linv;
-  if (!L.parts) {
-    for (int r = tid; r < P.Np; r += NT) {
-      int I = r >> 3;
-      double dg = GT[(I * (I + 1) / 2 + I) * 64 + ak(r & 7, r & 7)];
-      scale[r] = (dg > 0.0) ? 1.0 / sqrt(dg) : 1.0;
-    }
-    __syncthreads();
-    for (int e = tid; e < P.ngt * 64; e += NT) {
-      int tau = e >> 6, idx = e & 63;
-      int I = tri_row(tau), J = tau - I * (I + 1) / 2;
-      int r = (idx >> 2) & 7, c = (idx >> 5) * 4 + (idx & 3);
-      GT[e] *= scale[I * 8 + r] * scale[J * 8 + c];
-    }
-    __syncthreads();
-    tile_cholesky(GT, P.NBT, P.NBT, flag_s, 1);
-    // unscale rows: L(i, j) /= s_i
-    for (int e = tid; e < P.ngt * 64; e += NT) {
-      int tau = e >> 6, idx = e & 63;
-      int I = tri_row(tau);
-      int r = (idx >> 2) & 7;
-      GT[e] /= scale[I * 8 + r];
-    }
-    __syncthreads();
-    // inverses of the diagonal tiles (column per lane)
-    for (int k = warp; k < P.NBT; k += DPG_NWARPS) {
-      const double* Lkk = GT + (k * (k + 1) / 2 + k) * 64;
-      double* X = LINV + k * 64;
-      if (lane < 8) {
-        const int c = lane;
-        double x[8];
-#pragma unroll
-        for (int r = 0; r < 8; r++) {
-          double v = (r == c) ? 1.0 : 0.0;
-#pragma unroll
-          for (int m = 0; m < r; m++) v -= Lkk[ak(r, m)] * x[m];
-          x[r] = (r < c) ? 0.0 : v / Lkk[ak(r, r)];
-        }
-#pragma unroll
-        for (int r = 0; r < 8; r++) X[ak(r, c)] = x[r];
-      }
-    }
-    __syncthreads();
-  }
-
-  // ======================= 3. B and F, one trial tile column per warp ========
+  for (int q = tid; q < P.nbpts; q += NT)
+    point_geometry(d, nv, X.nodes, P.dNB + (size_t)q * nv * d, P.wB[q], q >= P.QB ? P.tangB + (size_t)q * 6 : nullptr,
+                   geo + q * GEO);
   const int J = warp;
   const bool has_col = J < P.MBT;
   double2 bacc[NBTM];
 #pragma unroll
   for (int i = 0; i < NBTM; i++) bacc[i] = make_double2(0.0, 0.0);
-  if (L.solve_only) {
-    if (has_col) {
+  int gc = 0;  // global chunk counter (buffer parity)
+  for (int sgi = first_seg; sgi < P.nseg; sgi++) {
+    const DpgSeg& S = P.seg[sgi];
+    if (S.nterm == 0) continue;
+    for (int c = 0; c < S.nchunk; c++, gc++) {
+      const int buf = gc & 1;
+      double* rec = sm + (buf ? P.b_rec1 : P.b_rec0);
+      __syncthreads();  // the other buffer, U and R are free; geometry is complete
+      if (tid == 0) {
+        // prefetch the next chunk (this segment or the next one with terms)
+        int ns = sgi, nc = c + 1;
+        if (nc >= S.nchunk) {
+          ns = sgi + 1;
+          nc = 0;
+          while (ns < P.nseg && P.seg[ns].nterm == 0) ns++;
+        }
+        if (ns < P.nseg) {
+          const DpgSeg& S2 = P.seg[ns];
+          const uint32_t bytes = (uint32_t)(S2.chunk * S2.rec_len * sizeof(double));
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_expect_tx(&X.mbar[2 + (buf ^ 1)], bytes);
+          bulk_g2s(sm + (buf ? P.b_rec0 : P.b_rec1), S2.rec + (size_t)nc * S2.chunk * S2.rec_len, bytes,
+                   &X.mbar[2 + (buf ^ 1)]);
+        }
+      }
+      const int q0 = c * S.chunk;
+      const int nq = min(S.chunk, S.npts - q0);
+      // term rows R[lq][lt][4] = w*|J| * coef * slot * (n) * (parity) * T_op
+      for (int task = tid; task < S.chunk * S.nterm; task += NT) {
+        const int lq = task / S.nterm, lt = task - lq * S.nterm;
+        double* r = R + task * 4;
+        if (lq >= nq) { r[0] = r[1] = r[2] = r[3] = 0.0; continue; }
+        const int q = q0 + lq;
+        const DpgBTerm& Tm = P.bterm[S.term0 + lt];
+        const double* gq = geo + (S.geo0 + q) * GEO;
+        double v = gq[19] * Tm.coef;
+        if (Tm.slot >= 0) v *= X.coef[Tm.slot * P.Ptot + S.pbase + q];
+        if (Tm.normal_comp >= 0) v *= gq[20 + Tm.normal_comp];
+        if (Tm.kind == DPG_VAR_FLUX) v *= (double)par_c[S.side];
+        double tr[4];
+        trow_op(P.test[Tm.test_var].space, d, Tm.test_op, gq, tr);
+        r[0] = v * tr[0]; r[1] = v * tr[1]; r[2] = v * tr[2]; r[3] = v * tr[3];
+      }
+      if (!mbar_wait(&X.mbar[2 + buf], X.phase[2 + buf] & 1)) {
+        if (tid == 0) X.flag[2] = 1;
+      }
+      X.phase[2 + buf]++;
+      __syncthreads();
+      // U blocks: U[lq][blk][m][col] = sum over the block's terms of R[lq][lt][m] * trial value
+      for (int task = tid; task < S.chunk * S.nblk * 8; task += NT) {
+        const int lq = task / (S.nblk * 8);
+        const int rem = task - lq * S.nblk * 8;
+        const int kb = rem >> 3, cl = rem & 7;
+        const DpgBBlock& Bk = S.blk[kb];
+        const int col = Bk.J * 8 + cl;
+        const double* rq = rec + lq * S.rec_len;
+        double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
+        for (int i = 0; i < Bk.nt; i++) {
+          const int lt = Bk.terms[i];
+          const DpgBTerm& Tm = P.bterm[S.term0 + lt];
+          const int mm = col - Tm.col0;
+          if (mm < 0 || mm >= Tm.ncol) continue;
+          const double val = rq[S.tvoff[lt] + mm];
+          const double* r = R + (lq * S.nterm + lt) * 4;
+          u0 += r[0] * val; u1 += r[1] * val; u2 += r[2] * val; u3 += r[3] * val;
+        }
+        double* uq = U + lq * S.ustride + Bk.off + cl;
+        uq[0] = u0; uq[DPG_ULD] = u1; uq[2 * DPG_ULD] = u2; uq[3 * DPG_ULD] = u3;
+      }
+      __syncthreads();
+      if (has_col) {
+        for (int kb = 0; kb < S.nblk; kb++) {
+          const DpgBBlock& Bk = S.blk[kb];
+          if (Bk.J != J) continue;
+          const DpgTestVar& V = P.test[Bk.var];
+          const int i0 = V.ntile0, i1 = V.ntile0 + V.ntiles;
+#pragma unroll 1
+          for (int lq = 0; lq < nq; lq++) {
+            const double bfr = U[lq * S.ustride + Bk.off + t * DPG_ULD + g];
+            const double* abase = rec + lq * S.rec_len + V.foff + t * V.ldA + g - i0 * 8;
+#pragma unroll
+            for (int I = 0; I < NBTM; I++)
+              if (I >= i0 && I < i1) dmma(bacc[I], abase[I * 8], bfr);
+          }
+        }
+      }
+    }
+  }
+  if (!has_col) return;
+  if (L.parts) {
+    double* Bc = L.B ? L.B + (size_t)cell * P.M * P.N : nullptr;
+    double* Fc = L.F ? L.F + (size_t)cell * P.N : nullptr;
+#pragma unroll
+    for (int I = 0; I < NBTM; I++) {
+      if (I < P.NBT) {
+        int ur = P.dev2user_test[I * 8 + g];
+        if (ur >= 0) {
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            int col = J * 8 + 2 * t + e;
+            double v = e ? bacc[I].y : bacc[I].x;
+            int uc = P.dev2user_trial[col];
+            if (Bc && uc >= 0) Bc[(size_t)uc * P.N + ur] = v;
+            if (Fc && col == P.fcol) Fc[ur] = v;
+          }
+        }
+      }
+    }
+    return;
+  }
+  double2* scr = reinterpret_cast<double2*>(L.scratch + (size_t)blockIdx.x * P.scratch_per_cta) +
+                 (size_t)J * P.NBT * 32 + lane;
+#pragma unroll
+  for (int I = 0; I < NBTM; I++)
+    if (I < P.NBT) scr[I * 32] = bacc[I];
+}
+
+// ---------------------------------------------------------------------------
+// Phase 2: Gram matrix -> lower tiles in shared memory
+// ---------------------------------------------------------------------------
+template <int GTM>
+__device__ __noinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int d = P.d, nv = P.nv;
+  double* sm = X.sm;
+  double* geo = sm + P.g_geo;
+  double* Dm = sm + P.g_D;  // [q][pair][16]
+  double* hb = sm + P.g_h;
+  double* GT = sm + P.sm_gt;
+  const int nch = P.QGpad / DPG_CHG;
+  const uint32_t chunk_bytes = (uint32_t)(DPG_CHG * P.featstride * sizeof(double));
+  if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&X.mbar[0], chunk_bytes);
+    bulk_g2s(sm + P.g_fref0, P.frefG, chunk_bytes, &X.mbar[0]);
+  }
+  for (int q = tid; q < P.QGpad; q += NT)
+    point_geometry(d, nv, X.nodes, P.dNG + (size_t)q * nv * d, P.wG[q], nullptr, geo + q * GEO);
+  __syncthreads();
+  // coupling D_ab[k][l] = wdet * sum_r beta_r,a[k] beta_r,b[l],
+  // beta_r,a[k] = sum over row-r entries on var a of coef * slot * T_a[slot_e][k]
+  for (int task = tid; task < P.QGpad * P.npairs * 16; task += NT) {
+    const int q = task / (P.npairs * 16);
+    const int rem = task - q * P.npairs * 16;
+    const int p = rem >> 4, k = (rem >> 2) & 3, l = rem & 3;
+    const int a = P.pair_a[p], b = P.pair_b[p];
+    const double* gq = geo + q * GEO;
+    const int sa = P.test[a].space, sb = P.test[b].space;
+    double s = 0.0, ba = 0.0, bb = 0.0;
+    int row = P.nipent > 0 ? P.ipent[0].row : 0;
+    for (int e = 0; e < P.nipent; e++) {
+      const DpgIPEnt& E = P.ipent[e];
+      if (E.row != row) {
+        s += ba * bb;
+        ba = bb = 0.0;
+        row = E.row;
+      }
+      const int var = E.gslot >> 2, sl = E.gslot & 3;
+      if (var != a && var != b) continue;
+      double v = E.coef;
+      if (E.slot >= 0) v *= (q < P.QG) ? X.coef[E.slot * P.Ptot + q] : 0.0;
+      double tr[4];
+      if (var == a) {
+        trow_slot(sa, d, sl, gq, tr);
+        ba += v * tr[k];
+      }
+      if (var == b) {
+        trow_slot(sb, d, sl, gq, tr);
+        bb += v * tr[l];
+      }
+    }
+    s += ba * bb;
+    Dm[task] = s * gq[19];
+  }
+  // owned tiles
+  const int per = (P.ngt + DPG_NWARPS - 1) / DPG_NWARPS;
+  const int tau0 = warp * per;
+  const int ntw = max(0, min(per, P.ngt - tau0));
+  uint32_t pk[GTM];
+#pragma unroll
+  for (int u = 0; u < GTM; u++) {
+    uint32_t v = 0;
+    if (u < ntw) {
+      const DpgGTile T = X.tiles[tau0 + u];
+      v = (uint32_t)(T.aoff + t * T.lda + g) | ((uint32_t)(T.boff + t * T.ldb + g) << 16);
+    }
+    pk[u] = v;
+  }
+  double2 acc[GTM];
+#pragma unroll
+  for (int u = 0; u < GTM; u++) acc[u] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int c = 0; c < nch; c++) {
+    const int buf = c & 1;
+    const double* fref = sm + (buf ? P.g_fref1 : P.g_fref0);
+    if (tid == 0 && c + 1 < nch) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&X.mbar[buf ^ 1], chunk_bytes);
+      bulk_g2s(sm + (buf ? P.g_fref0 : P.g_fref1), P.frefG + (size_t)(c + 1) * DPG_CHG * P.featstride, chunk_bytes,
+               &X.mbar[buf ^ 1]);
+    }
+    if (!mbar_wait(&X.mbar[buf], X.phase[buf] & 1)) {
+      if (tid == 0) X.flag[2] = 1;
+    }
+    X.phase[buf]++;
+    // h_{b->a}[q][k][j] = sum_l D[k][l] slots_b[q][l][j]
+    {
+      const int per_q = P.hstride >> 2;  // sum over pairs of ldA_b
+      for (int task = tid; task < DPG_CHG * per_q; task += NT) {
+        const int lq = task / per_q;
+        const int jj = task - lq * per_q;
+        int p = 0;
+        while (p + 1 < P.npairs && (P.hoff[p + 1] >> 2) <= jj) p++;
+        const int b = P.pair_b[p];
+        const int ld = P.test[b].ldA;
+        const int j = jj - (P.hoff[p] >> 2);
+        const double* fb = fref + lq * P.featstride + P.test[b].foff + j;
+        const double f0 = fb[0], f1 = fb[ld], f2 = fb[2 * ld], f3 = fb[3 * ld];
+        const double* Dq = Dm + ((c * DPG_CHG + lq) * P.npairs + p) * 16;
+        double* hq = hb + lq * P.hstride + P.hoff[p] + j;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          hq[k * ld] = Dq[k * 4] * f0 + Dq[k * 4 + 1] * f1 + Dq[k * 4 + 2] * f2 + Dq[k * 4 + 3] * f3;
+      }
+    }
+    __syncthreads();
+    // DMMA over the owned tiles: one k-step (4 slots) per point
+#pragma unroll 1
+    for (int lq = 0; lq < DPG_CHG; lq++) {
+      const double* fa = fref + lq * P.featstride;
+      const double* hq = hb + lq * P.hstride;
+      uint32_t prevA = 0xffffffffu;
+      double afr = 0.0;
+#pragma unroll
+      for (int u = 0; u < GTM; u++) {
+        if (u < ntw) {
+          const uint32_t ao = pk[u] & 0xffffu;
+          if (ao != prevA) { afr = fa[ao]; prevA = ao; }
+          dmma(acc[u], afr, hq[pk[u] >> 16]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // accumulators -> tile-lower shared storage (overlaps the staging area)
+#pragma unroll
+  for (int u = 0; u < GTM; u++)
+    if (u < ntw) *reinterpret_cast<double2*>(GT + (tau0 + u) * 64 + ak_cfrag(g, t)) = acc[u];
+  __syncthreads();
+  // padded rows decouple: unit diagonal
+  for (int r = tid; r < P.Np; r += NT)
+    if (P.dev2user_test[r] < 0) GT[((r >> 3) * ((r >> 3) + 1) / 2 + (r >> 3)) * 64 + ak(r & 7, r & 7)] = 1.0;
+  __syncthreads();
+  if (L.parts && L.G) {
+    double* Gc = L.G + (size_t)cell * P.N * P.N;
+    for (int e = tid; e < P.Np * P.Np; e += NT) {
+      int r = e / P.Np, c2 = e - r * P.Np;
+      int ur = P.dev2user_test[r], uc = P.dev2user_test[c2];
+      if (ur >= 0 && uc >= 0) Gc[(size_t)ur * P.N + uc] = sym_get(GT, r, c2);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Phase 3: equilibrated Cholesky of G and inverses of its diagonal tiles
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void phase_factor(const DpgPlanDev& P, const Ctx& X) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  double* GT = X.sm + P.sm_gt;
+  double* scale = X.sm + P.sm_scale;
+  double* LINV = X.sm + P.sm_linv;
+  for (int r = tid; r < P.Np; r += NT) {
+    int I = r >> 3;
+    double dg = GT[(I * (I + 1) / 2 + I) * 64 + ak(r & 7, r & 7)];
+    scale[r] = (dg > 0.0) ? rsqrt(dg) : 1.0;
+  }
+  __syncthreads();
+  for (int u = warp; u < P.ngt; u += DPG_NWARPS) {
+    int ij = X.tri[u];
+    int I = ij & 255, J = ij >> 8;
+    double2* p = reinterpret_cast<double2*>(GT + u * 64 + ak_cfrag(g, t));
+    double si = scale[I * 8 + g];
+    double2 v = *p;
+    v.x *= si * scale[J * 8 + 2 * t];
+    v.y *= si * scale[J * 8 + 2 * t + 1];
+    *p = v;
+  }
+  __syncthreads();
+  tile_cholesky(GT, P.NBT, P.NBT, X.flag, 1, X.tri, X.invd);
+  // unscale rows: L(i, j) = Lscaled(i, j) / s_i ;  1 / L(i, i) = s_i / Lscaled(i, i)
+  for (int u = warp; u < P.ngt; u += DPG_NWARPS) {
+    int I = X.tri[u] & 255;
+    double2* p = reinterpret_cast<double2*>(GT + u * 64 + ak_cfrag(g, t));
+    double si = 1.0 / scale[I * 8 + g];
+    double2 v = *p;
+    v.x *= si;
+    v.y *= si;
+    *p = v;
+  }
+  for (int r = tid; r < P.Np; r += NT) X.invd[r] *= scale[r];
+  __syncthreads();
+  // inverses of the diagonal tiles (one column per lane)
+  for (int k = warp; k < P.NBT; k += DPG_NWARPS) {
+    const double* Lkk = GT + (k * (k + 1) / 2 + k) * 64;
+    double* Y = LINV + k * 64;
+    if (lane < 8) {
+      const int c = lane;
+      double x[8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        double v = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+        for (int m = 0; m < r; m++) v -= Lkk[ak(r, m)] * x[m];
+        x[r] = (r < c) ? 0.0 : v * X.invd[k * 8 + r];
+      }
+#pragma unroll
+      for (int r = 0; r < 8; r++) Y[ak(r, c)] = x[r];
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Phase 4: W = L^-1 [B | F] per column tile in registers, W^T tiles to smem
+// ---------------------------------------------------------------------------
+template <int NBTM>
+__device__ __noinline__ void phase_trsm(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const double* GT = X.sm + P.sm_gt;
+  const double* LINV = X.sm + P.sm_linv;
+  const int J = warp;
+  const bool has_col = J < P.MBT;
+  double2 bacc[NBTM];
+#pragma unroll
+  for (int i = 0; i < NBTM; i++) bacc[i] = make_double2(0.0, 0.0);
+  if (has_col) {
+    if (L.solve_only) {
       const double* Bc = L.Bin + (size_t)cell * P.M * P.N;
       const double* Fc = L.Fin + (size_t)cell * P.N;
 #pragma unroll
@@ -445,160 +716,13 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
           bacc[I] = make_double2(v[0], v[1]);
         }
       }
+    } else {
+      const double2* scr = reinterpret_cast<const double2*>(L.scratch + (size_t)blockIdx.x * P.scratch_per_cta) +
+                           (size_t)J * P.NBT * 32 + lane;
+#pragma unroll
+      for (int I = 0; I < NBTM; I++)
+        if (I < P.NBT) bacc[I] = scr[I * 32];
     }
-  } else {
-    double* geo = sm + P.sm_misc;
-    double* bops = sm + P.sm_bops;
-    double* bval = sm + P.sm_bval;
-    for (int sgi = 0; sgi < P.nseg; sgi++) {
-      const DpgSeg& S = P.seg[sgi];
-      if (S.nterm == 0) continue;
-      const int side = sgi - 1;
-      for (int q0 = 0; q0 < S.npts; q0 += DPG_CHUNK) {
-        const int np = min(DPG_CHUNK, S.npts - q0);
-        __syncthreads();
-        if (tid < DPG_CHUNK) {
-          double* gq = geo + tid * 32;
-          if (tid < np) {
-            Geo G;
-            const double* dN = (side < 0) ? P.dNB + (size_t)(q0 + tid) * nv * d
-                                          : P.dNS + ((size_t)side * P.QS + q0 + tid) * nv * d;
-            geometry(d, nv, nodes_s, dN, G);
-#pragma unroll
-            for (int i = 0; i < 9; i++) { gq[i] = G.J[i]; gq[9 + i] = G.Ji[i]; }
-            gq[18] = G.det;
-            if (side < 0) {
-              gq[19] = P.wB[q0 + tid] * G.det;
-              gq[21] = gq[22] = gq[23] = 0.0;
-            } else {
-              const double* Tq = P.sideT + ((size_t)side * P.QS + q0 + tid) * 6;
-              double T0[3] = {0, 0, 0}, T1[3] = {0, 0, 0};
-              for (int i = 0; i < d; i++)
-                for (int j = 0; j < d; j++) {
-                  T0[i] += G.J[i * 3 + j] * Tq[j];
-                  T1[i] += G.J[i * 3 + j] * Tq[3 + j];
-                }
-              double meas, n[3];
-              if (d == 2) {
-                meas = sqrt(T0[0] * T0[0] + T0[1] * T0[1]);
-                n[0] = T0[1] / meas; n[1] = -T0[0] / meas; n[2] = 0.0;
-              } else {
-                double c0 = T0[1] * T1[2] - T0[2] * T1[1];
-                double c1 = T0[2] * T1[0] - T0[0] * T1[2];
-                double c2 = T0[0] * T1[1] - T0[1] * T1[0];
-                meas = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
-                n[0] = c0 / meas; n[1] = c1 / meas; n[2] = c2 / meas;
-              }
-              gq[19] = P.wS[q0 + tid] * meas;
-              gq[21] = n[0]; gq[22] = n[1]; gq[23] = n[2];
-            }
-          } else {
-#pragma unroll
-            for (int i = 0; i < 9; i++) { gq[i] = (i % 4 == 0) ? 1.0 : 0.0; gq[9 + i] = gq[i]; }
-            gq[18] = 1.0;
-            gq[19] = 0.0;
-            gq[21] = gq[22] = gq[23] = 0.0;
-          }
-        }
-        __syncthreads();
-        // stage test ops [op][q][ldA]
-        for (int o = 0; o < S.nops; o++) {
-          const DpgBOp& O = S.ops[o];
-          const DpgTestVar& V = P.test[O.var];
-          const int n = DPG_CHUNK * V.ldA;
-          double* dst = bops + O.off;
-          for (int i = tid; i < n; i += NT) {
-            int q = i / V.ldA, row = i - q * V.ldA;
-            double v = 0.0;
-            if (q < np && row < V.card) {
-              const double* ref = (side < 0)
-                  ? V.tabB + ((size_t)(q0 + q) * V.card + row) * V.nref
-                  : V.tabS + (((size_t)side * P.QS + q0 + q) * V.card + row) * V.nref;
-              v = test_op(V.space, d, O.op, ref, geo + q * 32);
-            }
-            dst[i] = v;
-          }
-        }
-        // stage weighted trial values [term][q][ldT]
-        for (int tt = 0; tt < S.nterm; tt++) {
-          const DpgBTerm& Tm = P.bterm[S.term0 + tt];
-          double* dst = bval + tt * DPG_CHUNK * P.ldT;
-          for (int i = tid; i < DPG_CHUNK * P.ldT; i += NT) {
-            int q = i / P.ldT, m = i - q * P.ldT;
-            double v = 0.0;
-            int mm = m - Tm.col0;
-            if (q < np && mm >= 0 && mm < Tm.ncol) {
-              const double* gq = geo + q * 32;
-              double w = gq[19] * Tm.coef;
-              if (Tm.slot >= 0) {
-                int pidx = (side < 0) ? P.QG + q0 + q : P.QG + P.QB + side * P.QS + q0 + q;
-                w *= coef_c[(size_t)Tm.slot * P.Ptot + pidx];
-              }
-              if (Tm.normal_comp >= 0) w *= gq[21 + Tm.normal_comp];
-              if (Tm.kind < 0) {
-                v = w;  // RHS: the F column
-              } else {
-                const DpgTrialVar& TV = P.trial[Tm.trial_var];
-                double val;
-                if (Tm.kind == DPG_VAR_FIELD) {
-                  val = (side < 0) ? TV.tabB[(size_t)(q0 + q) * TV.card_comp + mm]
-                                   : TV.tabS[((size_t)side * P.QS + q0 + q) * TV.card_comp + mm];
-                } else {
-                  val = TV.tabS[(size_t)(q0 + q) * TV.per_side + mm];
-                  if (Tm.kind == DPG_VAR_FLUX) w *= (double)par_c[side];
-                }
-                v = w * val;
-              }
-            }
-            dst[i] = v;
-          }
-        }
-        __syncthreads();
-        if (has_col) {
-          for (int tt = 0; tt < S.nterm; tt++) {
-            const DpgBTerm& Tm = P.bterm[S.term0 + tt];
-            if (Tm.col0 >= J * 8 + 8 || Tm.col0 + Tm.ncol <= J * 8) continue;
-            const DpgBOp& O = S.ops[Tm.bop];
-            const DpgTestVar& V = P.test[O.var];
-            const double bfr = bval[(tt * DPG_CHUNK + t) * P.ldT + J * 8 + g];
-            const double* abase = bops + O.off + t * V.ldA + g - V.ntile0 * 8;
-            const int i0 = V.ntile0, i1 = V.ntile0 + V.ntiles;
-#pragma unroll
-            for (int I = 0; I < NBTM; I++)
-              if (I >= i0 && I < i1) dmma(bacc[I], abase[I * 8], bfr);
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
-
-  if (L.parts) {
-    if (has_col) {
-      double* Bc = L.B ? L.B + (size_t)cell * P.M * P.N : nullptr;
-      double* Fc = L.F ? L.F + (size_t)cell * P.N : nullptr;
-#pragma unroll
-      for (int I = 0; I < NBTM; I++) {
-        if (I < P.NBT) {
-          int ur = P.dev2user_test[I * 8 + g];
-          if (ur >= 0) {
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-              int col = J * 8 + 2 * t + e;
-              double v = e ? bacc[I].y : bacc[I].x;
-              int uc = P.dev2user_trial[col];
-              if (Bc && uc >= 0) Bc[(size_t)uc * P.N + ur] = v;
-              if (Fc && col == P.fcol) Fc[ur] = v;
-            }
-          }
-        }
-      }
-    }
-    return;
-  }
-
-  // ======================= 4. W = L^-1 [B | F] in registers ===================
-  if (has_col) {
 #pragma unroll
     for (int k = 0; k < NBTM; k++) {
       if (k < P.NBT) {
@@ -625,8 +749,8 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
     }
   }
   __syncthreads();
-  // W^T tiles (trial J, test I) in AK layout
-  double* WT = sm + P.sm_w;
+  // W^T tiles (trial J, test I) in AK layout (overlaps L: all warps are done with it)
+  double* WT = X.sm + P.sm_w;
   if (has_col) {
 #pragma unroll
     for (int I = 0; I < NBTM; I++) {
@@ -638,8 +762,16 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
     }
   }
   __syncthreads();
+}
 
-  // ======================= 5. K_ext = W^T W (lower tiles) =====================
+// ---------------------------------------------------------------------------
+// Phase 5/6: K_ext = W^T W, outputs, condensation
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const double* WT = X.sm + P.sm_w;
+  double* KT = X.sm + P.sm_k;
   {
     const int nk = P.MBT * (P.MBT + 1) / 2;
     const int per = (nk + DPG_NWARPS - 1) / DPG_NWARPS;
@@ -650,10 +782,9 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
 #pragma unroll
     for (int u = 0; u < DPG_MAX_KT; u++) {
       kacc[u] = make_double2(0.0, 0.0);
-      int tau = k0 + u;
-      int I = tri_row(tau);
-      kI[u] = I;
-      kJ[u] = tau - I * (I + 1) / 2;
+      int ij = (u < nkw) ? X.tri[k0 + u] : 0;
+      kI[u] = ij & 255;
+      kJ[u] = ij >> 8;
     }
     for (int R = 0; R < P.NBT; R++) {
 #pragma unroll
@@ -671,21 +802,20 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
       }
     }
     __syncthreads();
-    double* KT = sm + P.sm_k;
 #pragma unroll
     for (int u = 0; u < DPG_MAX_KT; u++)
       if (u < nkw) *reinterpret_cast<double2*>(KT + (k0 + u) * 64 + ak_cfrag(g, t)) = kacc[u];
     __syncthreads();
   }
-  double* KT = sm + P.sm_k;
   // K and l out (user numbering; fields first: dev = i for i < nf, nfp + (i - nf) otherwise)
   if (L.K) {
     double* Kc = L.K + (size_t)cell * P.M * P.M;
-    for (int e = tid; e < P.M * P.M; e += NT) {
-      int i = e / P.M, j = e - i * P.M;
-      int di = i < P.nf ? i : P.nfp + (i - P.nf);
-      int dj = j < P.nf ? j : P.nfp + (j - P.nf);
-      Kc[e] = sym_get(KT, di, dj);
+    for (int i = warp; i < P.M; i += DPG_NWARPS) {
+      const int di = i < P.nf ? i : P.nfp + (i - P.nf);
+      for (int j = lane; j < P.M; j += 32) {
+        const int dj = j < P.nf ? j : P.nfp + (j - P.nf);
+        Kc[(size_t)i * P.M + j] = sym_get(KT, di, dj);
+      }
     }
     double* lc = L.l + (size_t)cell * P.M;
     for (int i = tid; i < P.M; i += NT) {
@@ -693,63 +823,176 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
       lc[i] = sym_get(KT, P.fcol, di);
     }
   }
-  // ======================= 6. condensation ===================================
-  if (L.S && P.nfb > 0 && P.nt > 0) {
-    __syncthreads();
-    for (int r = P.nf + tid; r < P.nfp; r += NT) {
-      int I = r >> 3;
-      KT[(I * (I + 1) / 2 + I) * 64 + ak(r & 7, r & 7)] = 1.0;
+  if (L.S && P.nt > 0) {
+    if (P.nfb > 0) {
+      __syncthreads();
+      for (int r = P.nf + tid; r < P.nfp; r += NT) {
+        int I = r >> 3;
+        KT[(I * (I + 1) / 2 + I) * 64 + ak(r & 7, r & 7)] = 1.0;
+      }
+      __syncthreads();
+      tile_cholesky(KT, P.MBT, P.nfb, X.flag + 1, -1, X.tri, X.invd);
     }
-    __syncthreads();
-    tile_cholesky(KT, P.MBT, P.nfb, flag_s + 1, -1);
     double* Sc = L.S + (size_t)cell * P.nt * P.nt;
-    for (int e = tid; e < P.nt * P.nt; e += NT) {
-      int i = e / P.nt, j = e - i * P.nt;
-      Sc[e] = sym_get(KT, P.nfp + i, P.nfp + j);
-    }
+    for (int i = warp; i < P.nt; i += DPG_NWARPS)
+      for (int j = lane; j < P.nt; j += 32) Sc[(size_t)i * P.nt + j] = sym_get(KT, P.nfp + i, P.nfp + j);
     double* sc = L.s + (size_t)cell * P.nt;
     for (int i = tid; i < P.nt; i += NT) sc[i] = sym_get(KT, P.fcol, P.nfp + i);
-  } else if (L.S && P.nt > 0) {
-    double* Sc = L.S + (size_t)cell * P.nt * P.nt;
-    for (int e = tid; e < P.nt * P.nt; e += NT) {
-      int i = e / P.nt, j = e - i * P.nt;
-      Sc[e] = sym_get(KT, P.nfp + i, P.nfp + j);
-    }
-    double* sc = L.s + (size_t)cell * P.nt;
-    for (int i = tid; i < P.nt; i += NT) sc[i] = sym_get(KT, P.fcol, P.nfp + i);
-  }
-  __syncthreads();
-  if (tid == 0 && L.info) {
-    int f0 = flag_s[0], f1 = flag_s[1];
-    int v = 0;
-    if (f0 != 0) {
-      // device test row -> user test index (1-based)
-      int r = f0 - 1;
-      int u = L.solve_only ? r : P.dev2user_test[r];
-      v = (u >= 0 ? u : r) + 1;
-    } else if (f1 != 0) {
-      v = f1;
-    }
-    L.info[cell] = v;
   }
 }
+
+template <int NBTM, int GTM>
+__global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
+  extern __shared__ __align__(128) double sm[];
+  const int tid = threadIdx.x;
+  Ctx X;
+  X.sm = sm;
+  double* nodes_s = sm + P.sm_nodes;
+  X.nodes = nodes_s;
+  X.flag = reinterpret_cast<int*>(sm + P.sm_nodes + 24);
+  X.mbar = reinterpret_cast<uint64_t*>(sm + P.sm_nodes + 26);
+  int* tri_s = reinterpret_cast<int*>(sm + P.sm_nodes + 32);
+  X.tri = tri_s;
+  DpgGTile* tiles_s = reinterpret_cast<DpgGTile*>(sm + P.sm_tiles);
+  X.tiles = tiles_s;
+  double* coef_s = sm + P.sm_coef;
+  X.coef = coef_s;
+  X.invd = sm + P.sm_invd;
+  uint32_t phase[4] = {0, 0, 0, 0};
+  X.phase = phase;
+
+  // per-CTA set-up: triangular index table, tile table, mbarriers
+  const int ntri = DPG_MAX_NBT * (DPG_MAX_NBT + 1) / 2;
+  for (int u = tid; u < ntri; u += NT) {
+    int I = (int)((sqrt(8.0 * u + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= u) I++;
+    while (I * (I + 1) / 2 > u) I--;
+    tri_s[u] = I | ((u - I * (I + 1) / 2) << 8);
+  }
+  if (!L.solve_only)
+    for (int u = tid; u < P.ngt; u += NT) tiles_s[u] = P.gtiles[u];
+  if (tid == 0) {
+    for (int i = 0; i < 4; i++) mbar_init(&X.mbar[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  for (int cell = blockIdx.x; cell < L.C; cell += gridDim.x) {
+    if (tid == 0) { X.flag[0] = 0; X.flag[1] = 0; X.flag[2] = 0; }
+    if (!L.solve_only) {
+      if (tid < P.nv * P.d) nodes_s[tid] = L.nodes[(size_t)cell * P.nv * P.d + tid];
+      const int nco = P.nslots * P.Ptot;
+      if (L.coeff)
+        for (int i = tid; i < nco; i += NT) coef_s[i] = L.coeff[(size_t)cell * nco + i];
+    }
+    __syncthreads();
+    double* GT = sm + P.sm_gt;
+    if (L.solve_only) {
+      const double* Gc = L.Gin + (size_t)cell * P.N * P.N;
+      for (int e = tid; e < P.ngt * 64; e += NT) {
+        int tau = e >> 6, idx = e & 63;
+        int ij = tri_s[tau];
+        int I = ij & 255, J = ij >> 8;
+        int r = (idx >> 2) & 7, c = (idx >> 5) * 4 + (idx & 3);
+        int gr = I * 8 + r, gc = J * 8 + c;
+        double v = 0.0;
+        if (gr < P.N && gc < P.N) v = Gc[(size_t)gr * P.N + gc];
+        else if (gr == gc) v = 1.0;
+        GT[e] = v;
+      }
+      __syncthreads();
+    } else {
+      phase_b<NBTM>(P, L, cell, X);
+      __syncthreads();
+      phase_gram<GTM>(P, L, cell, X);
+      if (L.parts) {
+        __syncthreads();
+        continue;
+      }
+    }
+    phase_factor(P, X);
+    phase_trsm<NBTM>(P, L, cell, X);
+    phase_syrk_out(P, L, cell, X);
+    __syncthreads();
+    if (tid == 0 && L.info) {
+      int f0 = X.flag[0], f1 = X.flag[1];
+      int v = 0;
+      if (X.flag[2]) {
+        v = ERR_TIMEOUT_FLAG;
+      } else if (f0 != 0) {
+        int r = f0 - 1;
+        int u = L.solve_only ? r : P.dev2user_test[r];
+        v = (u >= 0 ? u : r) + 1;
+      } else if (f1 != 0) {
+        v = f1;
+      }
+      L.info[cell] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// Instances: register arrays sized for the test-tile count of the bucket.
+#define DPG_INSTANCES(X) X(8, 3) X(12, 5) X(16, 9) X(18, 11) X(20, 14) X(22, 16) X(24, 19)
+
+typedef void (*KernelFn)(const DpgPlanDev, const DpgLaunch);
+
+static KernelFn pick_kernel(const DpgPlanDev* plan) {
+  const int per = (plan->ngt + DPG_NWARPS - 1) / DPG_NWARPS;
+#define DPG_PICK(NB, GT) \
+  if (plan->NBT <= NB && per <= GT) return dpg_cell_kernel<NB, GT>;
+  DPG_INSTANCES(DPG_PICK)
+#undef DPG_PICK
+  return nullptr;
+}
+
+static int g_num_sms = 0;
 
 }  // namespace
 
 int dpg_configure_kernels(const DpgPlanDev* plan) {
+  KernelFn k = pick_kernel(plan);
+  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
   size_t bytes = (size_t)plan->sm_total * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(dpg_cell_kernel<DPG_MAX_NBT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)bytes);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 1;
+    // keep freed stream-ordered scratch in the pool between calls
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+  }
   return DPG_OK;
 }
 
-int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const DpgLaunch* L, cudaStream_t stream) {
+int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const DpgLaunch* Lin, cudaStream_t stream) {
   (void)d_plan;
-  if (L->C <= 0) return DPG_OK;
+  if (Lin->C <= 0) return DPG_OK;
+  KernelFn k = pick_kernel(plan);
+  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
+  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  DpgLaunch L = *Lin;
+  void* scratch = nullptr;
+  const bool need_scratch = !L.solve_only && !L.parts && plan->scratch_per_cta > 0 && !L.scratch;
+  if (need_scratch) {
+    cudaError_t ea = cudaMallocAsync(&scratch, (size_t)grid * plan->scratch_per_cta * sizeof(double), stream);
+    if (ea != cudaSuccess) {
+      cudaGetLastError();
+      return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(ea));
+    }
+    L.scratch = (double*)scratch;
+  }
   size_t bytes = (size_t)plan->sm_total * sizeof(double);
-  dpg_cell_kernel<DPG_MAX_NBT><<<L->C, NT, bytes, stream>>>(*plan, *L);
+  k<<<grid, NT, bytes, stream>>>(*plan, L);
   cudaError_t e = cudaGetLastError();
+  if (scratch) cudaFreeAsync(scratch, stream);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
 }

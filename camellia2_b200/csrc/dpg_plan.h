@@ -6,44 +6,76 @@
 //    to a multiple of 8 ("trial tiles").  The F column (the load vector) rides
 //    along as one extra trial column so y = L^-1 F and l = W^T y fall out of the
 //    same triangular solve and Gram product as W and K.
+//  * Reference features: every test var has four "slots" per dof and point,
+//    HGRAD: (phi, dphi/dxi_0, dphi/dxi_1, dphi/dxi_2), HDIV: (v_0, .., v_{d-1}, div v)
+//    (unused slots zero).  Physical operators are linear in the slots with
+//    per-point coefficients from the Jacobian (the Piola maps), so every
+//    geometric factor is folded into small per-point coupling matrices and the
+//    slot tables themselves are per-bucket constants, copied to shared memory
+//    by bulk (TMA) copies.  Staged layout per point: [var][slot][ldA].
 //  * 8x8 tiles in shared memory use the "AK" layout: element (r, c) of a tile is at
 //    ((c >> 2) * 8 + r) * 4 + (c & 3).  A-fragments of mma.m8n8k4 (thread (g,t)
 //    holds A[g][4h+t]) and B-fragments of the transposed tile then read 32
 //    consecutive doubles per k-step h: bank-conflict free.
 #pragma once
+#include <stdint.h>
 
 #define DPG_MAXV 8        // max test vars / trial vars per bucket
-#define DPG_MAX_BF 96     // max scalar bilinear products
+#define DPG_MAX_BF 96     // max scalar bilinear products (after side expansion)
 #define DPG_MAX_IP 64     // max inner-product entries
 #define DPG_MAX_RHS 8
-#define DPG_MAX_FEAT 32   // 4 features per test var (padded) * DPG_MAXV
 #define DPG_MAX_IPROWS 24
-#define DPG_MAX_BOPS 24   // distinct (test var, op) pairs used by B terms in a segment
 #define DPG_MAX_SEG 7     // volume + up to 6 sides
+#define DPG_MAX_BLK 24    // active (test var, trial column tile) blocks per segment
+#define DPG_MAX_PAIRS 36  // test var pairs a >= b
 #define DPG_NWARPS 16
 #define DPG_NTHREADS (DPG_NWARPS * 32)
-#define DPG_CHUNK 4       // quadrature points per staged chunk (one mma k-step per point)
+#define DPG_CHG 8         // Gram quadrature points per staged chunk
+#define DPG_MAX_CHB 16    // max B quadrature points per staged chunk
+#define DPG_MAX_BT 12     // max terms feeding one B block
+#define DPG_MAX_QG 512    // max Gram-rule points
 #define DPG_MAX_NBT 24    // max test tiles (N <= 192)
 #define DPG_MAX_MBT 16    // max trial tiles incl. the F tile (one column tile per warp)
 #define DPG_MAX_GT 19     // max lower G tiles per warp: ceil(24*25/2 / 16)
 #define DPG_MAX_KT 9      // max lower K_ext tiles per warp: ceil(16*17/2 / 16)
+#define DPG_ULD 12        // leading dim of a staged 8-column U block (conflict-free B-fragments)
 
 struct DpgIPEnt {
   int row;      // (term, comp) row
-  int gfeat;    // global feature index: var * 4 + local feature
+  int gslot;    // global physical slot: var * 4 + slot
   double coef;
-  int slot;
+  int slot;     // coefficient slot, or -1
 };
 
 struct DpgBTerm {
-  int trial_var, trial_op, test_var, test_op;
+  int trial_var, test_var, test_op;
+  int kind;       // trial var kind; -1 = RHS (the F column)
   double coef;
   int slot, normal_comp;
-  int seg;        // 0 = volume, 1 + s = side s
-  int bop;        // index of (test var, test op) in the segment's op table
   int col0, ncol; // device trial columns touched (contiguous)
-  int kind;       // trial var kind
-  int tvar_comp;  // component (vector fields), 0 otherwise
+};
+
+struct DpgBBlock {
+  int var;        // test var
+  int J;          // trial column tile
+  int off;        // offset of the block inside a point's U region (doubles)
+  int nt;         // terms feeding the block (segment-local indices)
+  int terms[DPG_MAX_BT];
+};
+
+struct DpgSeg {
+  int npts;                 // quadrature points
+  int chunk, nchunk;        // points per staged chunk, number of chunks (chunk * nchunk >= npts)
+  int side;                 // -1 volume, else side index
+  const double* rec;        // [nchunk * chunk][rec_len] per-point records: reference slots, then trial values
+  int rec_len;              // doubles per record (even)
+  int geo0;                 // first point of the segment in the all-B-points geometry list
+  int pbase;                // first coefficient point index of the segment
+  int nblk;
+  DpgBBlock blk[DPG_MAX_BLK];
+  int ustride;              // doubles per point of staged U blocks
+  int term0, nterm;         // range in the segment-sorted term list
+  int tvoff[DPG_MAX_BF / 4];// offset of each (segment-local) term's trial values inside a record
 };
 
 struct DpgTrialVar {
@@ -52,8 +84,8 @@ struct DpgTrialVar {
   int dev_off;    // first device trial column
   int user_off;   // first user trial index
   int per_side;   // traces: dofs per side
-  const double* tabB;  // fields: ref values at B points [QB][card_comp]
-  const double* tabS;  // fields: [ns][QS][card_comp]; traces: [QS][per_side]
+  const double* tabB;  // fields: ref values at B points [QBpad][card_comp]
+  const double* tabS;  // fields: [ns][QSpad][card_comp]; traces: [QSpad][per_side]
 };
 
 struct DpgTestVar {
@@ -62,33 +94,14 @@ struct DpgTestVar {
   int dev_off;    // first device row
   int user_off;
   int ntile0, ntiles;  // tile range
-  int nref;       // reference comps per dof: HGRAD 1 + d (value, grad), HDIV d + 1 (value, div)
-  int nfeat;      // G features (<= 4)
-  int feat_op[4];
-  int ldA;        // padded leading dimension of staged operands (== 4 mod 16)
-  const double* tabG;  // [QG][card][nref]
-  const double* tabB;  // [QB][card][nref]
-  const double* tabS;  // [ns][QS][card][nref]
+  int ldA;        // padded leading dimension of staged slot rows (== 4 mod 16)
+  int foff;       // offset of the var inside a point's staged slot block
 };
 
 struct DpgGTile {
-  int I, J;       // tile coordinates (I >= J)
-  int aoff, lda;  // A operand: offset inside a point's feature block, leading dim
-  int boff, ldb;  // B operand: offset inside a point's h block
-};
-
-struct DpgBOp {
-  int var, op;
-  int off;        // offset inside a point's staged B-op block
-};
-
-struct DpgSeg {
-  int npts;       // quadrature points (volume: QB; side: QS)
-  int nops;
-  DpgBOp ops[DPG_MAX_BOPS];
-  int opstride;   // doubles per point of staged test ops
-  int term0, nterm;  // range in the (segment-sorted) term list
-  int rhs;        // 1: volume segment also carries the RHS (F column)
+  int16_t I, J;
+  int16_t lda, ldb;
+  int aoff, boff;  // A operand / B operand offsets inside a point's feature / h block
 };
 
 struct DpgPlanDev {
@@ -99,38 +112,44 @@ struct DpgPlanDev {
   int nfb;                  // field tiles
   int fcol;                 // device column of F
   int QG, QB, QS, Ptot, nslots;
+  int QGpad, QBpad, QSpad;
   int ntest, ntrial;
   DpgTestVar test[DPG_MAXV];
   DpgTrialVar trial[DPG_MAXV];
   // Gram
-  int Ftot;                 // 4 * ntest
   int niprows, nipent;
   DpgIPEnt ipent[DPG_MAX_IP];
+  int npairs;
+  int pair_a[DPG_MAX_PAIRS], pair_b[DPG_MAX_PAIRS];
+  int hoff[DPG_MAX_PAIRS];  // offset of h_{b->a} inside a point's h block
   int ngt;                  // lower G tiles
   const DpgGTile* gtiles;   // [ngt]
-  int featstride;           // doubles per point of staged features (sum over vars of 4*ldA)
+  int featstride;           // doubles per point of staged slots (sum over vars of 4*ldA)
   int hstride;              // doubles per point of staged h blocks (sum over pairs)
-  int hoff[DPG_MAXV][DPG_MAXV];  // offset of h_{b->a} block inside a point's h block (a >= b)
+  const double* frefG;      // [QGpad][featstride]
+  const double* wG;         // [QGpad]
+  const double* dNG;        // [QGpad][nv][d]
   // B and F
   int nseg;
   DpgSeg seg[DPG_MAX_SEG];
   int nbterm;
   DpgBTerm bterm[DPG_MAX_BF];  // sorted by segment
-  int nrhs;
-  DpgIPEnt rhs[DPG_MAX_RHS];   // (unused row), gfeat = test var * 16 + op, coef, slot
-  int ldT;                     // leading dim of staged trial values (== 4 mod 16, >= Mp)
-  // geometry tables
-  const double* dNG;  // [QG][nv][d]
-  const double* dNB;  // [QB][nv][d]
-  const double* dNS;  // [ns][QS][nv][d]
-  const double* wG;   // [QG]
-  const double* wB;   // [QB]
-  const double* wS;   // [QS]
-  const double* sideT;  // [ns][QS][2][3] reference tangents (2D: one)
+  int nbpts;                // all B points: volume then sides
+  const double* dNB;        // [nbpts][nv][d]
+  const double* wB;         // [nbpts]
+  const double* tangB;      // [nbpts][6] reference side tangents (zero for volume points)
+  int max_rec, max_chunk, max_ustride, max_nterm;
   // index maps
   const int* dev2user_trial;  // [Mp] -> user trial index, or -1
   const int* dev2user_test;   // [Np] -> user test index, or -1
   // shared memory layout (doubles)
   int sm_total;
-  int sm_geo, sm_cmat, sm_feat, sm_h, sm_gt, sm_linv, sm_scale, sm_bops, sm_bval, sm_w, sm_k, sm_misc;
+  int sm_tiles;   // persistent: tile table copy
+  int sm_nodes;   // persistent: cell vertices, flags, mbarriers, triangular index table (192 doubles)
+  int sm_coef;    // per cell: coefficients [nslots][Ptot]
+  int g_fref0, g_fref1, g_h, g_geo, g_D;           // Gram phase
+  int sm_gt, sm_linv, sm_scale, sm_invd;           // factor
+  int b_rec0, b_rec1, b_u, b_geo, b_R;             // B phase
+  int sm_w, sm_k;                                  // solve / Gram of W
+  size_t scratch_per_cta;                          // doubles of B scratch per CTA
 };
