@@ -1024,6 +1024,26 @@ int dpg_assemble(dpg_plan* p, int C, const double* nodes, const int8_t* parity, 
   return dpg_launch_assemble(&p->hp.dev, p->hp.d_dev, &L, (cudaStream_t)stream);
 }
 
+int dpg_assemble_noalloc(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                         double* K, double* l, double* S, double* s, int32_t* info, void* stream, int flags) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!nodes || !parity || !info) return fail(DPG_ERR_INVALID_ARGUMENT, "nodes, parity and info are required");
+  if (p->hp.dev.nslots > 0 && !coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+  if (!(flags & DPG_FLAG_NO_K) && (!K || !l)) return fail(DPG_ERR_INVALID_ARGUMENT, "K and l required");
+  if (!(flags & DPG_FLAG_NO_CONDENSE) && (!S || !s)) return fail(DPG_ERR_INVALID_ARGUMENT, "S and s required");
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.nodes = nodes; L.parity = parity; L.coeff = coeff;
+  L.K = (flags & DPG_FLAG_NO_K) ? nullptr : K;
+  L.l = (flags & DPG_FLAG_NO_K) ? nullptr : l;
+  L.S = (flags & DPG_FLAG_NO_CONDENSE) ? nullptr : S;
+  L.s = (flags & DPG_FLAG_NO_CONDENSE) ? nullptr : s;
+  L.info = info;
+  return dpg_launch_assemble_noalloc(&p->hp.dev, &L, (cudaStream_t)stream);
+}
+
 int dpg_assemble_parts(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff, double* G,
                        double* B, double* F, void* stream) {
   if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");

@@ -42,3 +42,4 @@ int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d
                       cudaStream_t* streams, int C, const double* nodes, const int8_t* parity, const double* coeff,
                       double* K, double* l, double* S, double* s, int32_t* info, int flags);
 int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);
+int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);

@@ -996,3 +996,59 @@ int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const 
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free launch: the per-CTA scratch comes from a fixed device array
+// instead of a stream-ordered allocation.  32 MiB (4 Mi doubles) is enough for
+// one CTA per SM at the largest buckets of the single-CTA kernel that fit in it
+// (the 3D hex k=2 bucket needs 165 KiB per CTA).
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define DPG_NOALLOC_SCRATCH_DOUBLES ((size_t)4 << 20)
+
+static __device__ __align__(256) double g_noalloc_scratch[DPG_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {nullptr};  // device address of the array, per device ordinal
+}  // namespace
+
+int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
+  if (Lin->C <= 0) return DPG_OK;
+  KernelFn k = pick_kernel(plan);
+  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
+  if (plan->scratch_per_cta > DPG_NOALLOC_SCRATCH_DOUBLES)
+    return dpg::fail(DPG_ERR_UNSUPPORTED,
+                     "dpg_assemble_noalloc: the bucket needs more per-CTA scratch than the fixed 32 MiB array holds");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return dpg::fail(DPG_ERR_CUDA, "dpg_assemble_noalloc: no current CUDA device");
+  }
+  double* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return dpg::fail(DPG_ERR_CUDA, std::string("dpg_assemble_noalloc: cudaGetSymbolAddress: ") +
+                                           cudaGetErrorString(e));
+      }
+      g_noalloc_ptr[dev] = (double*)p;
+    }
+    base = g_noalloc_ptr[dev];
+  }
+  const size_t fit = plan->scratch_per_cta > 0 ? DPG_NOALLOC_SCRATCH_DOUBLES / plan->scratch_per_cta : (size_t)Lin->C;
+  int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  grid = (int)std::min<size_t>((size_t)grid, fit);
+  DpgLaunch L = *Lin;
+  L.scratch = base;
+  size_t bytes = (size_t)plan->sm_total * sizeof(double);
+  k<<<grid, NT, bytes, stream>>>(*plan, L);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}

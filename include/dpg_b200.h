@@ -233,6 +233,31 @@ typedef struct dpg_bucket_batch {
 
 int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags);
 
+/* dpg_assemble without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory while
+ * they assemble — an application whose GPU memory is already fully reserved by
+ * its own pool (a framework's caching allocator, or a pre-sized arena shared by
+ * several solver ranks), or a time-stepping loop that must not take allocation
+ * latency or an out-of-memory failure in the middle of a step.
+ * dpg_assemble takes its per-CTA scratch (the B tiles held between the B phase
+ * and the triangular solve) from a stream-ordered allocation; this variant
+ * uses a fixed 32 MiB array that the library reserves on every GPU that loads
+ * it, until the process exits.  Same arguments, outputs and errors as
+ * dpg_assemble, plus:
+ *   - the first call on a device looks the array up (cudaGetSymbolAddress) with
+ *     that device current; make that first call before any stream capture;
+ *   - buckets whose per-CTA scratch exceeds 32 MiB are rejected with
+ *     DPG_ERR_UNSUPPORTED; otherwise the launch uses as many CTAs as fit
+ *     (floor(32 MiB / per-CTA scratch), at most one per SM), so large buckets
+ *     run on fewer SMs;
+ *   - every call shares the one array: calls that overlap on the GPU (other
+ *     streams, other threads, other plans) race and must be serialised by the
+ *     caller.  The array keeps the last call's contents; every call writes the
+ *     scratch it reads, so nothing needs clearing. */
+int dpg_assemble_noalloc(dpg_plan* plan, int C, const double* nodes, const int8_t* parity,
+                         const double* coeff, double* K, double* l, double* S, double* s,
+                         int32_t* info, void* stream, int flags);
+
 /* Thread-local description of the last error. */
 const char* dpg_last_error_string(void);
 
