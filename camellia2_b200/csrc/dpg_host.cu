@@ -563,6 +563,10 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   std::stable_sort(g.ipent, g.ipent + g.nipent, [](const DpgIPEnt& x, const DpgIPEnt& y) { return x.row < y.row; });
   g.niprows = (int)rowid.size();
   if (g.niprows > DPG_MAX_IPROWS) return fail(DPG_ERR_UNSUPPORTED, "too many IP rows");
+  for (int r = 0, e = 0; r <= g.niprows; r++) {
+    while (e < g.nipent && g.ipent[e].row < r) e++;
+    g.rowstart[r] = e;
+  }
   // var pairs (a >= b), h block offsets
   {
     int off = 0, np = 0;
@@ -681,6 +685,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   // B points, per-point term rows R, coefficients
   const int budget = 232448 / 8 - 192 - 2 * ((g.ngt * (int)sizeof(DpgGTile) + 7) / 8) - 64 - g.Np - g.Mp - 64;
   g.max_rec = 0; g.max_chunk = 0; g.max_ustride = 0; g.max_nterm = 0;
+  std::vector<int4> btiles;
   for (int sg = 0; sg < g.nseg; sg++) {
     DpgSeg& S = g.seg[sg];
     S.side = sg - 1;
@@ -719,9 +724,25 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     if (S.term0 < 0) S.term0 = 0;
     S.ustride = off;
     S.rec_len = (tv + 1) & ~1;
+    S.tile0 = (int)btiles.size();
+    for (int kb = 0; kb < S.nblk; kb++) {
+      const DpgTestVar& V = g.test[S.blk[kb].var];
+      for (int I = V.ntile0; I < V.ntile0 + V.ntiles; I++) btiles.push_back(make_int4(I, S.blk[kb].J, kb, 0));
+    }
+    S.ntile = (int)btiles.size() - S.tile0;
+    if ((S.ntile + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_BTW)
+      return fail(DPG_ERR_UNSUPPORTED, "too many active B tiles in a segment");
     g.max_rec = std::max(g.max_rec, S.rec_len);
     g.max_ustride = std::max(g.max_ustride, S.ustride);
     g.max_nterm = std::max(g.max_nterm, S.nterm);
+  }
+  {
+    void* p = nullptr;
+    size_t nb = std::max<size_t>(1, btiles.size()) * sizeof(int4);
+    if (cudaMalloc(&p, nb) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
+    if (!btiles.empty()) cudaMemcpy(p, btiles.data(), btiles.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    P->allocs.push_back(p);
+    g.btiles = (const int4*)p;
   }
   // chunk size: all points of a side in one chunk when it fits; the volume in equal chunks
   {
@@ -782,7 +803,9 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     // Gram phase
     g.g_fref0 = o; o += al(DPG_CHG * g.featstride);
     g.g_fref1 = o; o += al(DPG_CHG * g.featstride);
-    g.g_h = o; o += al(DPG_CHG * g.hstride);
+    g.g_h = o;
+    g.g_beta = o;  // per-point IP rows in reference slots; dead before the first h chunk
+    o += al(std::max(DPG_CHG * g.hstride, g.QGpad * g.niprows * 4 * g.ntest));
     g.g_geo = o; o += al(g.QGpad * 24);
     g.g_D = o; o += al(g.QGpad * g.npairs * 16);
     int gphase = o;
@@ -804,6 +827,8 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     int wsz = g.MBT * g.NBT * 64;
     g.sm_k = 0;
     int ksz = g.MBT * (g.MBT + 1) / 2 * 64;
+    if (g.sm_linv < ksz || g.sm_linv + g.MBT * 64 > g.sm_linv + al(g.NBT * 64))
+      return fail(DPG_ERR_UNSUPPORTED, "trial tiles outnumber test tiles: condensation workspace overlaps K");
     int body = std::max(std::max(gphase, bphase), std::max(std::max(wsz, ksz), fphase));
     g.sm_coef = al(body);
     g.sm_tiles = g.sm_coef + al(std::max(1, g.nslots * g.Ptot));

@@ -33,15 +33,19 @@
 #include <algorithm>
 #include <cstring>
 
+// The CTA's dynamic shared memory; every shared pointer below is derived from it
+// so the compiler keeps shared-space (LDS/STS) addressing inside the phase functions.
+extern __shared__ __align__(128) double dpg_smem[];
+
 namespace {
 
 constexpr int NT = DPG_NTHREADS;
 constexpr int MBAR_SPIN_LIMIT = 1 << 22;
 constexpr int ERR_TIMEOUT_FLAG = 0x7fff0000;
-constexpr int GEO = 24;  // doubles per point geometry record: J(9) Ji(9) det w*|J| n(3) pad
+constexpr int GEO = 24;  // doubles per point geometry record: J(9) Ji(9) det w*|J| n(3) 1/det
 
 __device__ __forceinline__ void dmma(double2& c, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                : "+d"(c.x), "+d"(c.y)
                : "d"(a), "d"(b));
 }
@@ -166,6 +170,7 @@ __device__ __forceinline__ void point_geometry(int d, int nv, const double* __re
 #pragma unroll
   for (int i = 0; i < 9; i++) { gq[i] = J[i]; gq[9 + i] = Ji[i]; }
   gq[18] = det;
+  gq[23] = 1.0 / det;
   gq[20] = gq[21] = gq[22] = 0.0;
   if (!tang) {
     gq[19] = w * det;
@@ -207,7 +212,7 @@ __device__ __forceinline__ void trow_slot(int space, int d, int m, const double*
       for (int j = 0; j < d; j++) r[1 + j] = gq[9 + j * 3 + c];
     }
   } else {
-    double id = 1.0 / gq[18];
+    const double id = gq[23];
     if (m < d) {
       for (int j = 0; j < d; j++) r[j] = gq[m * 3 + j] * id;
     } else if (m == d) {
@@ -223,7 +228,7 @@ __device__ __forceinline__ void trow_op(int space, int d, int op, const double* 
     return;
   }
   if (op == DPG_OP_DOT_NORMAL) {
-    double id = 1.0 / gq[18];
+    const double id = gq[23];
     r[0] = r[1] = r[2] = r[3] = 0.0;
     for (int c = 0; c < d; c++)
       for (int j = 0; j < d; j++) r[j] += gq[20 + c] * gq[c * 3 + j] * id;
@@ -240,86 +245,129 @@ __device__ __forceinline__ double sym_get(const double* base, int r, int c) {
 }
 
 struct Ctx {
-  double* sm;
-  int* flag;        // [0] Gram pivot, [1] condensation pivot, [2] staging timeout
-  uint64_t* mbar;   // [0,1] Gram slots, [2,3] B records
-  const int* tri;   // lower tile index -> (I | J << 8)
-  const DpgGTile* tiles;
-  const double* nodes;
-  const double* coef;  // this cell's coefficients [nslots][Ptot]
-  double* invd;        // inverse pivots of the current factorisation
   uint32_t* phase;     // mbarrier use counters [4]
 };
 
-// Blocked right-looking Cholesky of the leading nsteps tiles of a tile-lower
-// matrix with nb tiles in shared memory.  invd[8k + j] receives 1 / L_jj.
-// Records the first failing global pivot (1-based) into *flag with sign `sgn`.
-__device__ __noinline__ void tile_cholesky(double* __restrict__ T, int nb, int nsteps, int* flag, int sgn,
-                                           const int* tri, double* invd) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  for (int k = 0; k < nsteps; k++) {
-    double* Tkk = T + (k * (k + 1) / 2 + k) * 64;
-    if (warp == 0) {
-      double row[8];
-      const int r = lane & 7;
+// Shared-memory views of the persistent region (derived from dpg_smem).
+#define DPG_SMEM_VIEWS(P)                                                              \
+  double* const sm = dpg_smem;                                                         \
+  int* const flag_s = reinterpret_cast<int*>(sm + (P).sm_nodes + 24);                  \
+  uint64_t* const mbar_s = reinterpret_cast<uint64_t*>(sm + (P).sm_nodes + 26);        \
+  const int* const tri_s = reinterpret_cast<const int*>(sm + (P).sm_nodes + 32);       \
+  const double* const nodes_s = sm + (P).sm_nodes;                                     \
+  const double* const coef_s = sm + (P).sm_coef;                                       \
+  double* const invd_s = sm + (P).sm_invd;                                             \
+  (void)flag_s; (void)mbar_s; (void)tri_s; (void)nodes_s; (void)coef_s; (void)invd_s;
+
+// Factor the diagonal tile k in place (one warp; lanes 0..7 hold rows), record
+// 1 / L_jj in invd[8k + j] and, when linv != nullptr, the inverse tile L_kk^-1
+// (AK layout) in linv[64 k].  First failing pivot (1-based) -> *flag (sign sgn).
+__device__ __forceinline__ void factor_diag(double* __restrict__ T, int k, int* flag, int sgn, double* invd,
+                                            double* linv) {
+  const int lane = threadIdx.x & 31;
+  double* Tkk = T + (k * (k + 1) / 2 + k) * 64;
+  double row[8];
+  const int r = lane & 7;
 #pragma unroll
-      for (int c = 0; c < 8; c++) row[c] = Tkk[ak(r, c)];
-      bool failed = false;
-      int fail_j = 0;
+  for (int c = 0; c < 8; c++) row[c] = Tkk[ak(r, c)];
+  bool failed = false;
+  int fail_j = 0;
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        double piv = __shfl_sync(0xffffffffu, row[j], j);
-        if (!(piv > 0.0) && !failed) { failed = true; fail_j = j; }
-        double inv = rsqrt(piv);
-        if (r == j) { row[j] = piv * inv; if (lane < 8) invd[k * 8 + j] = inv; }
-        else if (r > j) row[j] *= inv;
+  for (int j = 0; j < 8; j++) {
+    double piv = __shfl_sync(0xffffffffu, row[j], j);
+    if (!(piv > 0.0) && !failed) { failed = true; fail_j = j; }
+    double inv = rsqrt(piv);
+    if (r == j) { row[j] = piv * inv; if (lane < 8) invd[k * 8 + j] = inv; }
+    else if (r > j) row[j] *= inv;
 #pragma unroll
-        for (int c = j + 1; c < 8; c++) {
-          double lcj = __shfl_sync(0xffffffffu, row[j], c);
-          if (r >= c) row[c] -= row[j] * lcj;
-        }
-      }
-      if (lane < 8) {
-#pragma unroll
-        for (int c = 0; c < 8; c++) Tkk[ak(r, c)] = (c <= r) ? row[c] : 0.0;
-      }
-      if (lane == 0 && failed && *flag == 0) *flag = sgn * (k * 8 + fail_j + 1);
+    for (int c = j + 1; c < 8; c++) {
+      double lcj = __shfl_sync(0xffffffffu, row[j], c);
+      if (r >= c) row[c] -= row[j] * lcj;
     }
-    __syncthreads();
-    // panel: L_ik = A_ik L_kk^-T, one row per thread
-    const int nrows = (nb - 1 - k) * 8;
-    const double* iv = invd + k * 8;
-    for (int w = tid; w < nrows; w += NT) {
-      int i = k + 1 + (w >> 3), r = w & 7;
-      double* Tik = T + (i * (i + 1) / 2 + k) * 64;
+  }
+  if (lane < 8) {
+#pragma unroll
+    for (int c = 0; c < 8; c++) Tkk[ak(r, c)] = (c <= r) ? row[c] : 0.0;
+  }
+  if (lane == 0 && failed && *flag == 0) *flag = sgn * (k * 8 + fail_j + 1);
+  if (linv) {
+    __syncwarp();
+    // column c of L_kk^-1 by forward substitution (lane c)
+    if (lane < 8) {
+      const int c = lane;
       double x[8];
 #pragma unroll
-      for (int c = 0; c < 8; c++) x[c] = Tik[ak(r, c)];
+      for (int rr = 0; rr < 8; rr++) {
+        double v = (rr == c) ? 1.0 : 0.0;
 #pragma unroll
-      for (int c = 0; c < 8; c++) {
-        double v = x[c];
-#pragma unroll
-        for (int m = 0; m < c; m++) v -= x[m] * Tkk[ak(c, m)];
-        x[c] = v * iv[c];
+        for (int m = 0; m < rr; m++) v -= Tkk[ak(rr, m)] * x[m];
+        x[rr] = (rr < c) ? 0.0 : v * invd[k * 8 + rr];
       }
 #pragma unroll
-      for (int c = 0; c < 8; c++) Tik[ak(r, c)] = x[c];
+      for (int rr = 0; rr < 8; rr++) linv[k * 64 + ak(rr, c)] = x[rr];
+    }
+    __syncwarp();
+  }
+}
+
+// Blocked right-looking Cholesky of the leading nsteps tiles of a tile-lower
+// matrix with nb tiles in shared memory (AK tiles).  Look-ahead: while warps
+// 1..15 apply the trailing update of step k, warp 0 updates diagonal tile k+1
+// first and factors it, so each step costs two barriers.  The panel multiplies by
+// the inverse diagonal tile (two DMMAs per tile).  linv (NBT x 64) receives the
+// inverses of the factored diagonal tiles; invd the inverse pivots.
+__device__ __noinline__ void tile_cholesky(int T_off, int nb, int nsteps, int flag_idx, int sgn, int tri_off,
+                                           int invd_off, int linv_off) {
+  double* const T = dpg_smem + T_off;
+  int* const flag = reinterpret_cast<int*>(dpg_smem) + flag_idx;
+  const int* const tri = reinterpret_cast<const int*>(dpg_smem + tri_off);
+  double* const invd = dpg_smem + invd_off;
+  double* const linv = dpg_smem + linv_off;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  if (nsteps <= 0) return;
+  if (warp == 0) factor_diag(T, 0, flag, sgn, invd, linv);
+  __syncthreads();
+  for (int k = 0; k < nsteps; k++) {
+    // panel: L_ik = A_ik L_kk^-T
+    const double* Li = linv + k * 64;
+    for (int i = k + 1 + warp; i < nb; i += DPG_NWARPS) {
+      double* Tik = T + (i * (i + 1) / 2 + k) * 64;
+      const double a0 = Tik[lane], a1 = Tik[32 + lane];
+      double2 c = make_double2(0.0, 0.0);
+      dmma(c, a0, Li[lane]);
+      dmma(c, a1, Li[32 + lane]);
+      __syncwarp();
+      *reinterpret_cast<double2*>(Tik + ak_cfrag(g, t)) = c;
     }
     __syncthreads();
-    // trailing update: A_ij -= L_ik L_jk^T for k < j <= i < nb
+    // trailing update: A_ij -= L_ik L_jk^T for k < j <= i < nb; warp 0 does (k+1, k+1) and factors it
     const int m = nb - 1 - k;
     const int ntr = m * (m + 1) / 2;
-    for (int u = warp; u < ntr; u += DPG_NWARPS) {
-      int ij = tri[u];
-      int i = k + 1 + (ij & 255), j = k + 1 + (ij >> 8);
-      double* Tij = T + (i * (i + 1) / 2 + j) * 64;
-      const double* Lik = T + (i * (i + 1) / 2 + k) * 64;
-      const double* Ljk = T + (j * (j + 1) / 2 + k) * 64;
-      double2 c = *reinterpret_cast<const double2*>(Tij + ak_cfrag(g, t));
-      dmma(c, -Lik[lane], Ljk[lane]);
-      dmma(c, -Lik[32 + lane], Ljk[32 + lane]);
-      *reinterpret_cast<double2*>(Tij + ak_cfrag(g, t)) = c;
+    if (warp == 0) {
+      if (m > 0) {
+        const int i = k + 1;
+        double* Tii = T + (i * (i + 1) / 2 + i) * 64;
+        const double* Lik = T + (i * (i + 1) / 2 + k) * 64;
+        double2 c = *reinterpret_cast<const double2*>(Tii + ak_cfrag(g, t));
+        dmma(c, -Lik[lane], Lik[lane]);
+        dmma(c, -Lik[32 + lane], Lik[32 + lane]);
+        *reinterpret_cast<double2*>(Tii + ak_cfrag(g, t)) = c;
+        __syncwarp();
+        if (k + 1 < nsteps) factor_diag(T, k + 1, flag, sgn, invd, linv);
+      }
+    } else {
+      for (int u = 1 + (warp - 1); u < ntr; u += DPG_NWARPS - 1) {
+        int ij = tri[u];
+        int i = k + 1 + (ij & 255), j = k + 1 + (ij >> 8);
+        double* Tij = T + (i * (i + 1) / 2 + j) * 64;
+        const double* Lik = T + (i * (i + 1) / 2 + k) * 64;
+        const double* Ljk = T + (j * (j + 1) / 2 + k) * 64;
+        double2 c = *reinterpret_cast<const double2*>(Tij + ak_cfrag(g, t));
+        dmma(c, -Lik[lane], Ljk[lane]);
+        dmma(c, -Lik[32 + lane], Ljk[32 + lane]);
+        *reinterpret_cast<double2*>(Tij + ak_cfrag(g, t)) = c;
+      }
     }
     __syncthreads();
   }
@@ -328,16 +376,17 @@ __device__ __noinline__ void tile_cholesky(double* __restrict__ T, int nb, int n
 // ---------------------------------------------------------------------------
 // Phase 1: B and F -> per-CTA scratch (or the B/F outputs in parts mode)
 // ---------------------------------------------------------------------------
-template <int NBTM>
-__device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+template <int BTW>
+__device__ __forceinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int d = P.d, nv = P.nv;
-  double* sm = X.sm;
+  DPG_SMEM_VIEWS(P);
   double* geo = sm + P.b_geo;
   double* U = sm + P.b_u;
   double* R = sm + P.b_R;
   const int8_t* par_c = L.parity + (size_t)cell * P.ns;
+  double2* scr = reinterpret_cast<double2*>(L.scratch + (size_t)blockIdx.x * P.scratch_per_cta);
   // prologue: first chunk's records in flight while the geometry is computed
   int first_seg = 0;
   while (first_seg < P.nseg && P.seg[first_seg].nterm == 0) first_seg++;
@@ -345,21 +394,36 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
     const DpgSeg& S = P.seg[first_seg];
     const uint32_t bytes = (uint32_t)(S.chunk * S.rec_len * sizeof(double));
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&X.mbar[2], bytes);
-    bulk_g2s(sm + P.b_rec0, S.rec, bytes, &X.mbar[2]);
+    mbar_expect_tx(&mbar_s[2], bytes);
+    bulk_g2s(sm + P.b_rec0, S.rec, bytes, &mbar_s[2]);
   }
+  // [B | F] tiles accumulate in this CTA's scratch slot, C-fragment layout per tile
+  for (int i = tid; i < P.MBT * P.NBT * 32; i += NT) scr[i] = make_double2(0.0, 0.0);
   for (int q = tid; q < P.nbpts; q += NT)
-    point_geometry(d, nv, X.nodes, P.dNB + (size_t)q * nv * d, P.wB[q], q >= P.QB ? P.tangB + (size_t)q * 6 : nullptr,
+    point_geometry(d, nv, nodes_s, P.dNB + (size_t)q * nv * d, P.wB[q], q >= P.QB ? P.tangB + (size_t)q * 6 : nullptr,
                    geo + q * GEO);
-  const int J = warp;
-  const bool has_col = J < P.MBT;
-  double2 bacc[NBTM];
-#pragma unroll
-  for (int i = 0; i < NBTM; i++) bacc[i] = make_double2(0.0, 0.0);
   int gc = 0;  // global chunk counter (buffer parity)
   for (int sgi = first_seg; sgi < P.nseg; sgi++) {
     const DpgSeg& S = P.seg[sgi];
     if (S.nterm == 0) continue;
+    // this warp's active tiles of the segment: operand offsets and accumulators
+    const int per = (S.ntile + DPG_NWARPS - 1) / DPG_NWARPS;
+    const int my0 = S.tile0 + warp * per;
+    const int nmine = max(0, min(per, S.tile0 + S.ntile - my0));
+    int aoff[BTW], boff[BTW];
+    double2 acc[BTW];
+#pragma unroll
+    for (int u = 0; u < BTW; u++) {
+      acc[u] = make_double2(0.0, 0.0);
+      aoff[u] = 0; boff[u] = 0;
+      if (u < nmine) {
+        const int4 td = P.btiles[my0 + u];
+        const DpgBBlock& Bk = S.blk[td.z];
+        const DpgTestVar& V = P.test[Bk.var];
+        aoff[u] = V.foff + t * V.ldA + (td.x - V.ntile0) * 8 + g;
+        boff[u] = Bk.off + t * DPG_ULD + g;
+      }
+    }
     for (int c = 0; c < S.nchunk; c++, gc++) {
       const int buf = gc & 1;
       double* rec = sm + (buf ? P.b_rec1 : P.b_rec0);
@@ -376,9 +440,9 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
           const DpgSeg& S2 = P.seg[ns];
           const uint32_t bytes = (uint32_t)(S2.chunk * S2.rec_len * sizeof(double));
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          mbar_expect_tx(&X.mbar[2 + (buf ^ 1)], bytes);
+          mbar_expect_tx(&mbar_s[2 + (buf ^ 1)], bytes);
           bulk_g2s(sm + (buf ? P.b_rec0 : P.b_rec1), S2.rec + (size_t)nc * S2.chunk * S2.rec_len, bytes,
-                   &X.mbar[2 + (buf ^ 1)]);
+                   &mbar_s[2 + (buf ^ 1)]);
         }
       }
       const int q0 = c * S.chunk;
@@ -392,15 +456,15 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
         const DpgBTerm& Tm = P.bterm[S.term0 + lt];
         const double* gq = geo + (S.geo0 + q) * GEO;
         double v = gq[19] * Tm.coef;
-        if (Tm.slot >= 0) v *= X.coef[Tm.slot * P.Ptot + S.pbase + q];
+        if (Tm.slot >= 0) v *= coef_s[Tm.slot * P.Ptot + S.pbase + q];
         if (Tm.normal_comp >= 0) v *= gq[20 + Tm.normal_comp];
         if (Tm.kind == DPG_VAR_FLUX) v *= (double)par_c[S.side];
         double tr[4];
         trow_op(P.test[Tm.test_var].space, d, Tm.test_op, gq, tr);
         r[0] = v * tr[0]; r[1] = v * tr[1]; r[2] = v * tr[2]; r[3] = v * tr[3];
       }
-      if (!mbar_wait(&X.mbar[2 + buf], X.phase[2 + buf] & 1)) {
-        if (tid == 0) X.flag[2] = 1;
+      if (tid == 0) {
+        if (!mbar_wait(&mbar_s[2 + buf], X.phase[2 + buf] & 1)) flag_s[2] = 1;
       }
       X.phase[2 + buf]++;
       __syncthreads();
@@ -426,62 +490,58 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
         uq[0] = u0; uq[DPG_ULD] = u1; uq[2 * DPG_ULD] = u2; uq[3 * DPG_ULD] = u3;
       }
       __syncthreads();
-      if (has_col) {
-        for (int kb = 0; kb < S.nblk; kb++) {
-          const DpgBBlock& Bk = S.blk[kb];
-          if (Bk.J != J) continue;
-          const DpgTestVar& V = P.test[Bk.var];
-          const int i0 = V.ntile0, i1 = V.ntile0 + V.ntiles;
+      // DMMA over this warp's active tiles of the segment: one k-step (4 slots) per point
 #pragma unroll 1
-          for (int lq = 0; lq < nq; lq++) {
-            const double bfr = U[lq * S.ustride + Bk.off + t * DPG_ULD + g];
-            const double* abase = rec + lq * S.rec_len + V.foff + t * V.ldA + g - i0 * 8;
+      for (int lq = 0; lq < nq; lq++) {
+        const double* ra = rec + lq * S.rec_len;
+        const double* ub = U + lq * S.ustride;
 #pragma unroll
-            for (int I = 0; I < NBTM; I++)
-              if (I >= i0 && I < i1) dmma(bacc[I], abase[I * 8], bfr);
-          }
-        }
+        for (int u = 0; u < BTW; u++)
+          if (u < nmine) dmma(acc[u], ra[aoff[u]], ub[boff[u]]);
+      }
+    }
+    // segment contributions into the scratch tiles (each tile has one owner per segment)
+#pragma unroll
+    for (int u = 0; u < BTW; u++) {
+      if (u < nmine) {
+        const int4 td = P.btiles[my0 + u];
+        const int si = (td.y * P.NBT + td.x) * 32 + lane;
+        double2 v = scr[si];
+        v.x += acc[u].x;
+        v.y += acc[u].y;
+        scr[si] = v;
       }
     }
   }
-  if (!has_col) return;
-  if (L.parts) {
-    double* Bc = L.B ? L.B + (size_t)cell * P.M * P.N : nullptr;
-    double* Fc = L.F ? L.F + (size_t)cell * P.N : nullptr;
+  if (!L.parts) return;
+  __syncthreads();
+  double* Bc = L.B ? L.B + (size_t)cell * P.M * P.N : nullptr;
+  double* Fc = L.F ? L.F + (size_t)cell * P.N : nullptr;
+  for (int tile = warp; tile < P.MBT * P.NBT; tile += DPG_NWARPS) {
+    const int J = tile / P.NBT, I = tile - J * P.NBT;
+    const double2 v = scr[tile * 32 + lane];
+    const int ur = P.dev2user_test[I * 8 + g];
+    if (ur < 0) continue;
 #pragma unroll
-    for (int I = 0; I < NBTM; I++) {
-      if (I < P.NBT) {
-        int ur = P.dev2user_test[I * 8 + g];
-        if (ur >= 0) {
-#pragma unroll
-          for (int e = 0; e < 2; e++) {
-            int col = J * 8 + 2 * t + e;
-            double v = e ? bacc[I].y : bacc[I].x;
-            int uc = P.dev2user_trial[col];
-            if (Bc && uc >= 0) Bc[(size_t)uc * P.N + ur] = v;
-            if (Fc && col == P.fcol) Fc[ur] = v;
-          }
-        }
-      }
+    for (int e = 0; e < 2; e++) {
+      const int col = J * 8 + 2 * t + e;
+      const double x = e ? v.y : v.x;
+      const int uc = P.dev2user_trial[col];
+      if (Bc && uc >= 0) Bc[(size_t)uc * P.N + ur] = x;
+      if (Fc && col == P.fcol) Fc[ur] = x;
     }
-    return;
   }
-  double2* scr = reinterpret_cast<double2*>(L.scratch + (size_t)blockIdx.x * P.scratch_per_cta) +
-                 (size_t)J * P.NBT * 32 + lane;
-#pragma unroll
-  for (int I = 0; I < NBTM; I++)
-    if (I < P.NBT) scr[I * 32] = bacc[I];
 }
 
 // ---------------------------------------------------------------------------
 // Phase 2: Gram matrix -> lower tiles in shared memory
 // ---------------------------------------------------------------------------
 template <int GTM>
-__device__ __noinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+__device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int d = P.d, nv = P.nv;
-  double* sm = X.sm;
+  DPG_SMEM_VIEWS(P);
   double* geo = sm + P.g_geo;
   double* Dm = sm + P.g_D;  // [q][pair][16]
   double* hb = sm + P.g_h;
@@ -490,96 +550,97 @@ __device__ __noinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch& L,
   const uint32_t chunk_bytes = (uint32_t)(DPG_CHG * P.featstride * sizeof(double));
   if (tid == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&X.mbar[0], chunk_bytes);
-    bulk_g2s(sm + P.g_fref0, P.frefG, chunk_bytes, &X.mbar[0]);
+    mbar_expect_tx(&mbar_s[0], chunk_bytes);
+    bulk_g2s(sm + P.g_fref0, P.frefG, chunk_bytes, &mbar_s[0]);
   }
   for (int q = tid; q < P.QGpad; q += NT)
-    point_geometry(d, nv, X.nodes, P.dNG + (size_t)q * nv * d, P.wG[q], nullptr, geo + q * GEO);
+    point_geometry(d, nv, nodes_s, P.dNG + (size_t)q * nv * d, P.wG[q], nullptr, geo + q * GEO);
   __syncthreads();
-  // coupling D_ab[k][l] = wdet * sum_r beta_r,a[k] beta_r,b[l],
   // beta_r,a[k] = sum over row-r entries on var a of coef * slot * T_a[slot_e][k]
+  double* beta = sm + P.g_beta;  // [q][row][4 * ntest]
+  const int F = 4 * P.ntest;
+  for (int task = tid; task < P.QGpad * P.niprows * P.ntest; task += NT) {
+    const int q = task / (P.niprows * P.ntest);
+    const int rem = task - q * P.niprows * P.ntest;
+    const int r = rem / P.ntest, a = rem - r * P.ntest;
+    const double* gq = geo + q * GEO;
+    double b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+    for (int e = P.rowstart[r]; e < P.rowstart[r + 1]; e++) {
+      const DpgIPEnt& E = P.ipent[e];
+      if ((E.gslot >> 2) != a) continue;
+      double v = E.coef;
+      if (E.slot >= 0) v *= (q < P.QG) ? coef_s[E.slot * P.Ptot + q] : 0.0;
+      double tr[4];
+      trow_slot(P.test[a].space, d, E.gslot & 3, gq, tr);
+      b0 += v * tr[0]; b1 += v * tr[1]; b2 += v * tr[2]; b3 += v * tr[3];
+    }
+    double* dst = beta + (q * P.niprows + r) * F + 4 * a;
+    dst[0] = b0; dst[1] = b1; dst[2] = b2; dst[3] = b3;
+  }
+  __syncthreads();
+  // coupling D_ab[k][l] = wdet * sum_r beta_r,a[k] beta_r,b[l]
   for (int task = tid; task < P.QGpad * P.npairs * 16; task += NT) {
     const int q = task / (P.npairs * 16);
     const int rem = task - q * P.npairs * 16;
     const int p = rem >> 4, k = (rem >> 2) & 3, l = rem & 3;
-    const int a = P.pair_a[p], b = P.pair_b[p];
-    const double* gq = geo + q * GEO;
-    const int sa = P.test[a].space, sb = P.test[b].space;
-    double s = 0.0, ba = 0.0, bb = 0.0;
-    int row = P.nipent > 0 ? P.ipent[0].row : 0;
-    for (int e = 0; e < P.nipent; e++) {
-      const DpgIPEnt& E = P.ipent[e];
-      if (E.row != row) {
-        s += ba * bb;
-        ba = bb = 0.0;
-        row = E.row;
-      }
-      const int var = E.gslot >> 2, sl = E.gslot & 3;
-      if (var != a && var != b) continue;
-      double v = E.coef;
-      if (E.slot >= 0) v *= (q < P.QG) ? X.coef[E.slot * P.Ptot + q] : 0.0;
-      double tr[4];
-      if (var == a) {
-        trow_slot(sa, d, sl, gq, tr);
-        ba += v * tr[k];
-      }
-      if (var == b) {
-        trow_slot(sb, d, sl, gq, tr);
-        bb += v * tr[l];
-      }
-    }
-    s += ba * bb;
-    Dm[task] = s * gq[19];
+    const double* bq = beta + q * P.niprows * F;
+    const int ia = 4 * P.pair_a[p] + k, ib = 4 * P.pair_b[p] + l;
+    double sacc = 0.0;
+    for (int r = 0; r < P.niprows; r++) sacc += bq[r * F + ia] * bq[r * F + ib];
+    Dm[task] = sacc * geo[q * GEO + 19];
   }
-  // owned tiles
+  // owned tiles: packed per-thread operand offsets (A | B << 16)
   const int per = (P.ngt + DPG_NWARPS - 1) / DPG_NWARPS;
   const int tau0 = warp * per;
   const int ntw = max(0, min(per, P.ngt - tau0));
+  const int4* tdesc = reinterpret_cast<const int4*>(sm + P.sm_tiles) + tau0;
   uint32_t pk[GTM];
+  double2 acc[GTM];
 #pragma unroll
   for (int u = 0; u < GTM; u++) {
+    acc[u] = make_double2(0.0, 0.0);
     uint32_t v = 0;
     if (u < ntw) {
-      const DpgGTile T = X.tiles[tau0 + u];
-      v = (uint32_t)(T.aoff + t * T.lda + g) | ((uint32_t)(T.boff + t * T.ldb + g) << 16);
+      const int4 T = tdesc[u];
+      v = (uint32_t)(T.z + t * (T.y & 0xffff) + g) | ((uint32_t)(T.w + t * (T.y >> 16) + g) << 16);
     }
     pk[u] = v;
   }
-  double2 acc[GTM];
-#pragma unroll
-  for (int u = 0; u < GTM; u++) acc[u] = make_double2(0.0, 0.0);
+  // h work units per point: (pair, column tile of the pair's second var); warp w takes
+  // units w, w + 16, ... for every point of the chunk
+  int nunit = 0;
+  for (int p = 0; p < P.npairs; p++) nunit += P.test[P.pair_b[p]].ntiles;
   __syncthreads();
   for (int c = 0; c < nch; c++) {
     const int buf = c & 1;
     const double* fref = sm + (buf ? P.g_fref1 : P.g_fref0);
-    if (tid == 0 && c + 1 < nch) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(&X.mbar[buf ^ 1], chunk_bytes);
-      bulk_g2s(sm + (buf ? P.g_fref0 : P.g_fref1), P.frefG + (size_t)(c + 1) * DPG_CHG * P.featstride, chunk_bytes,
-               &X.mbar[buf ^ 1]);
-    }
-    if (!mbar_wait(&X.mbar[buf], X.phase[buf] & 1)) {
-      if (tid == 0) X.flag[2] = 1;
+    if (tid == 0) {
+      if (c + 1 < nch) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&mbar_s[buf ^ 1], chunk_bytes);
+        bulk_g2s(sm + (buf ? P.g_fref0 : P.g_fref1), P.frefG + (size_t)(c + 1) * DPG_CHG * P.featstride,
+                 chunk_bytes, &mbar_s[buf ^ 1]);
+      }
+      if (!mbar_wait(&mbar_s[buf], X.phase[buf] & 1)) flag_s[2] = 1;
     }
     X.phase[buf]++;
-    // h_{b->a}[q][k][j] = sum_l D[k][l] slots_b[q][l][j]
-    {
-      const int per_q = P.hstride >> 2;  // sum over pairs of ldA_b
-      for (int task = tid; task < DPG_CHG * per_q; task += NT) {
-        const int lq = task / per_q;
-        const int jj = task - lq * per_q;
-        int p = 0;
-        while (p + 1 < P.npairs && (P.hoff[p + 1] >> 2) <= jj) p++;
-        const int b = P.pair_b[p];
-        const int ld = P.test[b].ldA;
-        const int j = jj - (P.hoff[p] >> 2);
-        const double* fb = fref + lq * P.featstride + P.test[b].foff + j;
-        const double f0 = fb[0], f1 = fb[ld], f2 = fb[2 * ld], f3 = fb[3 * ld];
-        const double* Dq = Dm + ((c * DPG_CHG + lq) * P.npairs + p) * 16;
-        double* hq = hb + lq * P.hstride + P.hoff[p] + j;
+    __syncthreads();
+    // h_{b->a}[q] = D_q (4x4, padded to 8 rows) * slots_b[q] (4 x 8 column tile): one DMMA per unit and point
+    for (int un = warp; un < nunit; un += DPG_NWARPS) {
+      int r = un, p = 0;
+      while (r >= P.test[P.pair_b[p]].ntiles) { r -= P.test[P.pair_b[p]].ntiles; p++; }
+      const int b = P.pair_b[p];
+      const int ld = P.test[b].ldA;
+      const double* dp = Dm + ((size_t)c * DPG_CHG * P.npairs + p) * 16 + g * 4 + t;
+      const double* fp = fref + P.test[b].foff + t * ld + r * 8 + g;
+      double* hp = hb + P.hoff[p] + g * ld + r * 8 + 2 * t;
 #pragma unroll
-        for (int k = 0; k < 4; k++)
-          hq[k * ld] = Dq[k * 4] * f0 + Dq[k * 4 + 1] * f1 + Dq[k * 4 + 2] * f2 + Dq[k * 4 + 3] * f3;
+      for (int lq = 0; lq < DPG_CHG; lq++) {
+        const double av = (g < 4) ? dp[lq * P.npairs * 16] : 0.0;
+        const double bv = fp[lq * P.featstride];
+        double2 hc = make_double2(0.0, 0.0);
+        dmma(hc, av, bv);
+        if (g < 4) *reinterpret_cast<double2*>(hp + lq * P.hstride) = hc;
       }
     }
     __syncthreads();
@@ -589,13 +650,13 @@ __device__ __noinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch& L,
       const double* fa = fref + lq * P.featstride;
       const double* hq = hb + lq * P.hstride;
       uint32_t prevA = 0xffffffffu;
-      double afr = 0.0;
+      double av = 0.0;
 #pragma unroll
       for (int u = 0; u < GTM; u++) {
         if (u < ntw) {
           const uint32_t ao = pk[u] & 0xffffu;
-          if (ao != prevA) { afr = fa[ao]; prevA = ao; }
-          dmma(acc[u], afr, hq[pk[u] >> 16]);
+          if (ao != prevA) { av = fa[ao]; prevA = ao; }
+          dmma(acc[u], av, hq[pk[u] >> 16]);
         }
       }
     }
@@ -623,12 +684,13 @@ __device__ __noinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch& L,
 // ---------------------------------------------------------------------------
 // Phase 3: equilibrated Cholesky of G and inverses of its diagonal tiles
 // ---------------------------------------------------------------------------
-__device__ __noinline__ void phase_factor(const DpgPlanDev& P, const Ctx& X) {
+__device__ __forceinline__ void phase_factor(const DpgPlanDev& P, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  double* GT = X.sm + P.sm_gt;
-  double* scale = X.sm + P.sm_scale;
-  double* LINV = X.sm + P.sm_linv;
+  DPG_SMEM_VIEWS(P);
+  double* GT = sm + P.sm_gt;
+  double* scale = sm + P.sm_scale;
+  double* LINV = sm + P.sm_linv;
   for (int r = tid; r < P.Np; r += NT) {
     int I = r >> 3;
     double dg = GT[(I * (I + 1) / 2 + I) * 64 + ak(r & 7, r & 7)];
@@ -636,7 +698,7 @@ __device__ __noinline__ void phase_factor(const DpgPlanDev& P, const Ctx& X) {
   }
   __syncthreads();
   for (int u = warp; u < P.ngt; u += DPG_NWARPS) {
-    int ij = X.tri[u];
+    int ij = tri_s[u];
     int I = ij & 255, J = ij >> 8;
     double2* p = reinterpret_cast<double2*>(GT + u * 64 + ak_cfrag(g, t));
     double si = scale[I * 8 + g];
@@ -646,10 +708,10 @@ __device__ __noinline__ void phase_factor(const DpgPlanDev& P, const Ctx& X) {
     *p = v;
   }
   __syncthreads();
-  tile_cholesky(GT, P.NBT, P.NBT, X.flag, 1, X.tri, X.invd);
-  // unscale rows: L(i, j) = Lscaled(i, j) / s_i ;  1 / L(i, i) = s_i / Lscaled(i, i)
+  tile_cholesky(P.sm_gt, P.NBT, P.NBT, 2 * (P.sm_nodes + 24), 1, P.sm_nodes + 32, P.sm_invd, P.sm_linv);
+  // unscale: L = S^-1 Ls  (rows / s_i);  1 / L_ii = s_i / Ls_ii;  L_kk^-1 = Ls_kk^-1 S_k (columns * s_c)
   for (int u = warp; u < P.ngt; u += DPG_NWARPS) {
-    int I = X.tri[u] & 255;
+    int I = tri_s[u] & 255;
     double2* p = reinterpret_cast<double2*>(GT + u * 64 + ak_cfrag(g, t));
     double si = 1.0 / scale[I * 8 + g];
     double2 v = *p;
@@ -657,25 +719,11 @@ __device__ __noinline__ void phase_factor(const DpgPlanDev& P, const Ctx& X) {
     v.y *= si;
     *p = v;
   }
-  for (int r = tid; r < P.Np; r += NT) X.invd[r] *= scale[r];
-  __syncthreads();
-  // inverses of the diagonal tiles (one column per lane)
-  for (int k = warp; k < P.NBT; k += DPG_NWARPS) {
-    const double* Lkk = GT + (k * (k + 1) / 2 + k) * 64;
-    double* Y = LINV + k * 64;
-    if (lane < 8) {
-      const int c = lane;
-      double x[8];
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        double v = (r == c) ? 1.0 : 0.0;
-#pragma unroll
-        for (int m = 0; m < r; m++) v -= Lkk[ak(r, m)] * x[m];
-        x[r] = (r < c) ? 0.0 : v * X.invd[k * 8 + r];
-      }
-#pragma unroll
-      for (int r = 0; r < 8; r++) Y[ak(r, c)] = x[r];
-    }
+  for (int r = tid; r < P.Np; r += NT) invd_s[r] *= scale[r];
+  for (int e = tid; e < P.NBT * 64; e += NT) {
+    const int k = e >> 6, idx = e & 63;
+    const int c = (idx >> 5) * 4 + (idx & 3);
+    LINV[e] *= scale[k * 8 + c];
   }
   __syncthreads();
 }
@@ -687,8 +735,9 @@ template <int NBTM>
 __device__ __noinline__ void phase_trsm(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const double* GT = X.sm + P.sm_gt;
-  const double* LINV = X.sm + P.sm_linv;
+  DPG_SMEM_VIEWS(P);
+  const double* GT = sm + P.sm_gt;
+  const double* LINV = sm + P.sm_linv;
   const int J = warp;
   const bool has_col = J < P.MBT;
   double2 bacc[NBTM];
@@ -750,7 +799,7 @@ __device__ __noinline__ void phase_trsm(const DpgPlanDev& P, const DpgLaunch& L,
   }
   __syncthreads();
   // W^T tiles (trial J, test I) in AK layout (overlaps L: all warps are done with it)
-  double* WT = X.sm + P.sm_w;
+  double* WT = sm + P.sm_w;
   if (has_col) {
 #pragma unroll
     for (int I = 0; I < NBTM; I++) {
@@ -767,11 +816,12 @@ __device__ __noinline__ void phase_trsm(const DpgPlanDev& P, const DpgLaunch& L,
 // ---------------------------------------------------------------------------
 // Phase 5/6: K_ext = W^T W, outputs, condensation
 // ---------------------------------------------------------------------------
-__device__ __noinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+__device__ __forceinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const double* WT = X.sm + P.sm_w;
-  double* KT = X.sm + P.sm_k;
+  DPG_SMEM_VIEWS(P);
+  const double* WT = sm + P.sm_w;
+  double* KT = sm + P.sm_k;
   {
     const int nk = P.MBT * (P.MBT + 1) / 2;
     const int per = (nk + DPG_NWARPS - 1) / DPG_NWARPS;
@@ -782,7 +832,7 @@ __device__ __noinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLaunch
 #pragma unroll
     for (int u = 0; u < DPG_MAX_KT; u++) {
       kacc[u] = make_double2(0.0, 0.0);
-      int ij = (u < nkw) ? X.tri[k0 + u] : 0;
+      int ij = (u < nkw) ? tri_s[k0 + u] : 0;
       kI[u] = ij & 255;
       kJ[u] = ij >> 8;
     }
@@ -831,7 +881,7 @@ __device__ __noinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLaunch
         KT[(I * (I + 1) / 2 + I) * 64 + ak(r & 7, r & 7)] = 1.0;
       }
       __syncthreads();
-      tile_cholesky(KT, P.MBT, P.nfb, X.flag + 1, -1, X.tri, X.invd);
+      tile_cholesky(P.sm_k, P.MBT, P.nfb, 2 * (P.sm_nodes + 24) + 1, -1, P.sm_nodes + 32, P.sm_invd, P.sm_linv);
     }
     double* Sc = L.S + (size_t)cell * P.nt * P.nt;
     for (int i = warp; i < P.nt; i += DPG_NWARPS)
@@ -841,23 +891,17 @@ __device__ __noinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLaunch
   }
 }
 
-template <int NBTM, int GTM>
+template <int NBTM, int GTM, int BTW>
 __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
-  extern __shared__ __align__(128) double sm[];
   const int tid = threadIdx.x;
   Ctx X;
-  X.sm = sm;
+  double* const sm = dpg_smem;
   double* nodes_s = sm + P.sm_nodes;
-  X.nodes = nodes_s;
-  X.flag = reinterpret_cast<int*>(sm + P.sm_nodes + 24);
-  X.mbar = reinterpret_cast<uint64_t*>(sm + P.sm_nodes + 26);
+  int* flag_s = reinterpret_cast<int*>(sm + P.sm_nodes + 24);
+  uint64_t* mbar_s = reinterpret_cast<uint64_t*>(sm + P.sm_nodes + 26);
   int* tri_s = reinterpret_cast<int*>(sm + P.sm_nodes + 32);
-  X.tri = tri_s;
   DpgGTile* tiles_s = reinterpret_cast<DpgGTile*>(sm + P.sm_tiles);
-  X.tiles = tiles_s;
   double* coef_s = sm + P.sm_coef;
-  X.coef = coef_s;
-  X.invd = sm + P.sm_invd;
   uint32_t phase[4] = {0, 0, 0, 0};
   X.phase = phase;
 
@@ -872,13 +916,13 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
   if (!L.solve_only)
     for (int u = tid; u < P.ngt; u += NT) tiles_s[u] = P.gtiles[u];
   if (tid == 0) {
-    for (int i = 0; i < 4; i++) mbar_init(&X.mbar[i], 1);
+    for (int i = 0; i < 4; i++) mbar_init(&mbar_s[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
   for (int cell = blockIdx.x; cell < L.C; cell += gridDim.x) {
-    if (tid == 0) { X.flag[0] = 0; X.flag[1] = 0; X.flag[2] = 0; }
+    if (tid == 0) { flag_s[0] = 0; flag_s[1] = 0; flag_s[2] = 0; }
     if (!L.solve_only) {
       if (tid < P.nv * P.d) nodes_s[tid] = L.nodes[(size_t)cell * P.nv * P.d + tid];
       const int nco = P.nslots * P.Ptot;
@@ -902,7 +946,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
       }
       __syncthreads();
     } else {
-      phase_b<NBTM>(P, L, cell, X);
+      phase_b<BTW>(P, L, cell, X);
       __syncthreads();
       phase_gram<GTM>(P, L, cell, X);
       if (L.parts) {
@@ -915,9 +959,9 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
     phase_syrk_out(P, L, cell, X);
     __syncthreads();
     if (tid == 0 && L.info) {
-      int f0 = X.flag[0], f1 = X.flag[1];
+      int f0 = flag_s[0], f1 = flag_s[1];
       int v = 0;
-      if (X.flag[2]) {
+      if (flag_s[2]) {
         v = ERR_TIMEOUT_FLAG;
       } else if (f0 != 0) {
         int r = f0 - 1;
@@ -933,14 +977,17 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
 }
 
 // Instances: register arrays sized for the test-tile count of the bucket.
-#define DPG_INSTANCES(X) X(8, 3) X(12, 5) X(16, 9) X(18, 11) X(20, 14) X(22, 16) X(24, 19)
+#define DPG_INSTANCES(X) \
+  X(8, 3, 8) X(12, 5, 8) X(16, 9, 8) X(18, 11, 8) X(20, 14, 8) X(22, 16, 8) X(24, 19, 8) X(24, 19, 12)
 
 typedef void (*KernelFn)(const DpgPlanDev, const DpgLaunch);
 
 static KernelFn pick_kernel(const DpgPlanDev* plan) {
   const int per = (plan->ngt + DPG_NWARPS - 1) / DPG_NWARPS;
-#define DPG_PICK(NB, GT) \
-  if (plan->NBT <= NB && per <= GT) return dpg_cell_kernel<NB, GT>;
+  int btw = 0;
+  for (int s = 0; s < plan->nseg; s++) btw = std::max(btw, (plan->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
+#define DPG_PICK(NB, GT, BT) \
+  if (plan->NBT <= NB && per <= GT && btw <= BT) return dpg_cell_kernel<NB, GT, BT>;
   DPG_INSTANCES(DPG_PICK)
 #undef DPG_PICK
   return nullptr;
@@ -980,7 +1027,7 @@ int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const 
   const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
   DpgLaunch L = *Lin;
   void* scratch = nullptr;
-  const bool need_scratch = !L.solve_only && !L.parts && plan->scratch_per_cta > 0 && !L.scratch;
+  const bool need_scratch = !L.solve_only && plan->scratch_per_cta > 0 && !L.scratch;
   if (need_scratch) {
     cudaError_t ea = cudaMallocAsync(&scratch, (size_t)grid * plan->scratch_per_cta * sizeof(double), stream);
     if (ea != cudaSuccess) {

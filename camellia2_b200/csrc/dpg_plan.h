@@ -33,6 +33,7 @@
 #define DPG_CHG 8         // Gram quadrature points per staged chunk
 #define DPG_MAX_CHB 16    // max B quadrature points per staged chunk
 #define DPG_MAX_BT 12     // max terms feeding one B block
+#define DPG_MAX_BTW 12    // max active B tiles per warp per segment
 #define DPG_MAX_QG 512    // max Gram-rule points
 #define DPG_MAX_NBT 24    // max test tiles (N <= 192)
 #define DPG_MAX_MBT 16    // max trial tiles incl. the F tile (one column tile per warp)
@@ -76,6 +77,7 @@ struct DpgSeg {
   int ustride;              // doubles per point of staged U blocks
   int term0, nterm;         // range in the segment-sorted term list
   int tvoff[DPG_MAX_BF / 4];// offset of each (segment-local) term's trial values inside a record
+  int tile0, ntile;         // active (I, J) tiles of the segment: btiles[tile0 .. tile0 + ntile)
 };
 
 struct DpgTrialVar {
@@ -122,6 +124,7 @@ struct DpgPlanDev {
   int npairs;
   int pair_a[DPG_MAX_PAIRS], pair_b[DPG_MAX_PAIRS];
   int hoff[DPG_MAX_PAIRS];  // offset of h_{b->a} inside a point's h block
+  int rowstart[DPG_MAX_IPROWS + 1];  // IP entries of row r: [rowstart[r], rowstart[r+1])
   int ngt;                  // lower G tiles
   const DpgGTile* gtiles;   // [ngt]
   int featstride;           // doubles per point of staged slots (sum over vars of 4*ldA)
@@ -139,6 +142,7 @@ struct DpgPlanDev {
   const double* wB;         // [nbpts]
   const double* tangB;      // [nbpts][6] reference side tangents (zero for volume points)
   int max_rec, max_chunk, max_ustride, max_nterm;
+  const int4* btiles;       // active B tiles of all segments: (I, J, block, 0)
   // index maps
   const int* dev2user_trial;  // [Mp] -> user trial index, or -1
   const int* dev2user_test;   // [Np] -> user test index, or -1
@@ -147,7 +151,7 @@ struct DpgPlanDev {
   int sm_tiles;   // persistent: tile table copy
   int sm_nodes;   // persistent: cell vertices, flags, mbarriers, triangular index table (192 doubles)
   int sm_coef;    // per cell: coefficients [nslots][Ptot]
-  int g_fref0, g_fref1, g_h, g_geo, g_D;           // Gram phase
+  int g_fref0, g_fref1, g_h, g_geo, g_D, g_beta;   // Gram phase (g_beta overlaps g_h)
   int sm_gt, sm_linv, sm_scale, sm_invd;           // factor
   int b_rec0, b_rec1, b_u, b_geo, b_R;             // B phase
   int sm_w, sm_k;                                  // solve / Gram of W
