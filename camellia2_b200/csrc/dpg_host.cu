@@ -400,14 +400,16 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       if (n < 1) return fail(DPG_ERR_INVALID_ARGUMENT, "HDIV test order must be >= 1");
       tv.card = card_hdiv(d, n);
     } else return fail(DPG_ERR_INVALID_ARGUMENT, "test vars must be HGRAD or HDIV");
+    // rows padded to pairs of 8-row tiles (16x8 mma blocks never straddle two vars)
+    const int rows = (tv.card + 15) & ~15;
     tv.dev_off = dev_row;
     tv.user_off = user_row;
     tv.ntile0 = dev_row / 8;
-    tv.ntiles = pad8(tv.card) / 8;
-    tv.ldA = ld_pad(pad8(tv.card));
+    tv.ntiles = rows / 8;
+    tv.ldA = ld_pad(rows);
     tv.foff = foff;
     foff += 4 * tv.ldA;
-    dev_row += pad8(tv.card);
+    dev_row += rows;
     user_row += tv.card;
   }
   g.ntest = D->n_test;
@@ -583,23 +585,25 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     g.hstride = off;
     auto pair_index = [&](int a, int b) { return a * (a + 1) / 2 + b; };
     std::vector<DpgGTile> tiles;
-    for (int I = 0; I < g.NBT; I++)
-      for (int J = 0; J <= I; J++) {
-        int a = 0, b = 0;
-        for (int v = 0; v < g.ntest; v++) {
-          if (I >= g.test[v].ntile0 && I < g.test[v].ntile0 + g.test[v].ntiles) a = v;
-          if (J >= g.test[v].ntile0 && J < g.test[v].ntile0 + g.test[v].ntiles) b = v;
-        }
-        DpgGTile t;
-        t.I = (int16_t)I; t.J = (int16_t)J;
-        t.aoff = g.test[a].foff + (I - g.test[a].ntile0) * 8;
-        t.lda = (int16_t)g.test[a].ldA;
-        t.boff = g.hoff[pair_index(a, b)] + (J - g.test[b].ntile0) * 8;
-        t.ldb = (int16_t)g.test[b].ldA;
-        tiles.push_back(t);
+    for (int a = 0; a < g.ntest; a++)
+      for (int rp = 0; rp < g.test[a].ntiles; rp += 2) {
+        const int I = g.test[a].ntile0 + rp;
+        for (int b = 0; b <= a; b++)
+          for (int jj = 0; jj < g.test[b].ntiles; jj++) {
+            const int J = g.test[b].ntile0 + jj;
+            if (J > I + 1) continue;
+            DpgGTile t;
+            t.I = (int16_t)I; t.J = (int16_t)J;
+            t.aoff = g.test[a].foff + rp * 8;
+            t.lda = (int16_t)g.test[a].ldA;
+            t.boff = g.hoff[pair_index(a, b)] + jj * 8;
+            t.ldb = (int16_t)g.test[b].ldA;
+            tiles.push_back(t);
+          }
       }
-    g.ngt = (int)tiles.size();
-    if ((g.ngt + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_GT) return fail(DPG_ERR_UNSUPPORTED, "too many G tiles");
+    g.ngb = (int)tiles.size();
+    g.ngt = g.NBT * (g.NBT + 1) / 2;
+    if ((g.ngb + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_GT) return fail(DPG_ERR_UNSUPPORTED, "too many G blocks");
     void* p = nullptr;
     if (cudaMalloc(&p, tiles.size() * sizeof(DpgGTile)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
     cudaMemcpy(p, tiles.data(), tiles.size() * sizeof(DpgGTile), cudaMemcpyHostToDevice);
@@ -683,7 +687,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   }
   // shared-memory budget for the B phase: two record buffers, U, geometry of all
   // B points, per-point term rows R, coefficients
-  const int budget = 232448 / 8 - 192 - 2 * ((g.ngt * (int)sizeof(DpgGTile) + 7) / 8) - 64 - g.Np - g.Mp - 64;
+  const int budget = 232448 / 8 - 192 - 2 * ((g.ngb * (int)sizeof(DpgGTile) + 7) / 8) - 64 - g.Np - g.Mp - 64;
   g.max_rec = 0; g.max_chunk = 0; g.max_ustride = 0; g.max_nterm = 0;
   std::vector<int4> btiles;
   for (int sg = 0; sg < g.nseg; sg++) {
@@ -832,7 +836,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     int body = std::max(std::max(gphase, bphase), std::max(std::max(wsz, ksz), fphase));
     g.sm_coef = al(body);
     g.sm_tiles = g.sm_coef + al(std::max(1, g.nslots * g.Ptot));
-    g.sm_nodes = g.sm_tiles + al((g.ngt * (int)sizeof(DpgGTile) + 7) / 8);
+    g.sm_nodes = g.sm_tiles + al((g.ngb * (int)sizeof(DpgGTile) + 7) / 8);
     g.sm_invd = g.sm_nodes + 192;
     g.sm_total = g.sm_invd + al(std::max(g.Np, g.Mp));
     if ((size_t)g.sm_total * 8 > 232448)

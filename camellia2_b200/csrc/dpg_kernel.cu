@@ -50,6 +50,16 @@ __device__ __forceinline__ void dmma(double2& c, double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// D(16x8) += A(16x16) B(16x8), FP64.  Fragments: a[2i] = A[g][t+4i], a[2i+1] = A[g+8][t+4i],
+// b[i] = B[t+4i][g]; c = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
+__device__ __forceinline__ void dmma16(double* c, const double* a, const double* b) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
@@ -589,16 +599,16 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
     for (int r = 0; r < P.niprows; r++) sacc += bq[r * F + ia] * bq[r * F + ib];
     Dm[task] = sacc * geo[q * GEO + 19];
   }
-  // owned tiles: packed per-thread operand offsets (A | B << 16)
-  const int per = (P.ngt + DPG_NWARPS - 1) / DPG_NWARPS;
+  // owned 16x8 blocks: packed per-thread operand offsets (A | B << 16)
+  const int per = (P.ngb + DPG_NWARPS - 1) / DPG_NWARPS;
   const int tau0 = warp * per;
-  const int ntw = max(0, min(per, P.ngt - tau0));
+  const int ntw = max(0, min(per, P.ngb - tau0));
   const int4* tdesc = reinterpret_cast<const int4*>(sm + P.sm_tiles) + tau0;
   uint32_t pk[GTM];
-  double2 acc[GTM];
+  double acc[GTM][4];
 #pragma unroll
   for (int u = 0; u < GTM; u++) {
-    acc[u] = make_double2(0.0, 0.0);
+    acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
     uint32_t v = 0;
     if (u < ntw) {
       const int4 T = tdesc[u];
@@ -644,19 +654,29 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
       }
     }
     __syncthreads();
-    // DMMA over the owned tiles: one k-step (4 slots) per point
+    // m16n8k16 over the owned blocks: one k16 step = 4 points x 4 slots
 #pragma unroll 1
-    for (int lq = 0; lq < DPG_CHG; lq++) {
-      const double* fa = fref + lq * P.featstride;
-      const double* hq = hb + lq * P.hstride;
+    for (int s4 = 0; s4 < DPG_CHG; s4 += 4) {
+      const double* fa = fref + s4 * P.featstride;
+      const double* hq = hb + s4 * P.hstride;
       uint32_t prevA = 0xffffffffu;
-      double av = 0.0;
+      double av[8];
 #pragma unroll
       for (int u = 0; u < GTM; u++) {
         if (u < ntw) {
-          const uint32_t ao = pk[u] & 0xffffu;
-          if (ao != prevA) { av = fa[ao]; prevA = ao; }
-          dmma(acc[u], av, hq[pk[u] >> 16]);
+          const uint32_t ao = pk[u] & 0xffffu, bo = pk[u] >> 16;
+          if (ao != prevA) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              av[2 * i] = fa[i * P.featstride + ao];
+              av[2 * i + 1] = fa[i * P.featstride + ao + 8];
+            }
+            prevA = ao;
+          }
+          double bv[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) bv[i] = hq[i * P.hstride + bo];
+          dmma16(acc[u], av, bv);
         }
       }
     }
@@ -664,8 +684,16 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
   }
   // accumulators -> tile-lower shared storage (overlaps the staging area)
 #pragma unroll
-  for (int u = 0; u < GTM; u++)
-    if (u < ntw) *reinterpret_cast<double2*>(GT + (tau0 + u) * 64 + ak_cfrag(g, t)) = acc[u];
+  for (int u = 0; u < GTM; u++) {
+    if (u < ntw) {
+      const int4 T = tdesc[u];
+      const int I = T.x & 0xffff, J = T.x >> 16;
+      if (J <= I)
+        *reinterpret_cast<double2*>(GT + (I * (I + 1) / 2 + J) * 64 + ak_cfrag(g, t)) = make_double2(acc[u][0], acc[u][1]);
+      *reinterpret_cast<double2*>(GT + ((I + 1) * (I + 2) / 2 + J) * 64 + ak_cfrag(g, t)) =
+          make_double2(acc[u][2], acc[u][3]);
+    }
+  }
   __syncthreads();
   // padded rows decouple: unit diagonal
   for (int r = tid; r < P.Np; r += NT)
@@ -914,7 +942,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
     tri_s[u] = I | ((u - I * (I + 1) / 2) << 8);
   }
   if (!L.solve_only)
-    for (int u = tid; u < P.ngt; u += NT) tiles_s[u] = P.gtiles[u];
+    for (int u = tid; u < P.ngb; u += NT) tiles_s[u] = P.gtiles[u];
   if (tid == 0) {
     for (int i = 0; i < 4; i++) mbar_init(&mbar_s[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -978,12 +1006,12 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
 
 // Instances: register arrays sized for the test-tile count of the bucket.
 #define DPG_INSTANCES(X) \
-  X(8, 3, 8) X(12, 5, 8) X(16, 9, 8) X(18, 11, 8) X(20, 14, 8) X(22, 16, 8) X(24, 19, 8) X(24, 19, 12)
+  X(8, 3, 8) X(12, 5, 8) X(16, 6, 8) X(18, 8, 8) X(20, 8, 8) X(22, 9, 8) X(24, 12, 8) X(24, 12, 12)
 
 typedef void (*KernelFn)(const DpgPlanDev, const DpgLaunch);
 
 static KernelFn pick_kernel(const DpgPlanDev* plan) {
-  const int per = (plan->ngt + DPG_NWARPS - 1) / DPG_NWARPS;
+  const int per = (plan->ngb + DPG_NWARPS - 1) / DPG_NWARPS;
   int btw = 0;
   for (int s = 0; s < plan->nseg; s++) btw = std::max(btw, (plan->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
 #define DPG_PICK(NB, GT, BT) \

@@ -37,7 +37,7 @@
 #define DPG_MAX_QG 512    // max Gram-rule points
 #define DPG_MAX_NBT 24    // max test tiles (N <= 192)
 #define DPG_MAX_MBT 16    // max trial tiles incl. the F tile (one column tile per warp)
-#define DPG_MAX_GT 19     // max lower G tiles per warp: ceil(24*25/2 / 16)
+#define DPG_MAX_GT 12     // max 16x8 G blocks per warp
 #define DPG_MAX_KT 9      // max lower K_ext tiles per warp: ceil(16*17/2 / 16)
 #define DPG_ULD 12        // leading dim of a staged 8-column U block (conflict-free B-fragments)
 
@@ -100,6 +100,9 @@ struct DpgTestVar {
   int foff;       // offset of the var inside a point's staged slot block
 };
 
+// One 16x8 block of G for mma.m16n8k16: rows of test tiles (I, I+1) of one
+// var, columns of test tile J.  The upper tile (I, I+1) of a diagonal block is
+// computed and dropped.
 struct DpgGTile {
   int16_t I, J;
   int16_t lda, ldb;
@@ -125,8 +128,9 @@ struct DpgPlanDev {
   int pair_a[DPG_MAX_PAIRS], pair_b[DPG_MAX_PAIRS];
   int hoff[DPG_MAX_PAIRS];  // offset of h_{b->a} inside a point's h block
   int rowstart[DPG_MAX_IPROWS + 1];  // IP entries of row r: [rowstart[r], rowstart[r+1])
-  int ngt;                  // lower G tiles
-  const DpgGTile* gtiles;   // [ngt]
+  int ngt;                  // lower 8x8 tiles of G: NBT (NBT + 1) / 2
+  int ngb;                  // 16x8 G blocks
+  const DpgGTile* gtiles;   // [ngb]
   int featstride;           // doubles per point of staged slots (sum over vars of 4*ldA)
   int hstride;              // doubles per point of staged h blocks (sum over pairs)
   const double* frefG;      // [QGpad][featstride]
