@@ -614,6 +614,11 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   // ---- B terms, segments, RHS ----------------------------------------------
   if (D->n_rhs > DPG_MAX_RHS) return fail(DPG_ERR_UNSUPPORTED, "too many RHS terms");
   std::vector<std::pair<int, DpgBTerm>> terms;  // (segment, term)
+  std::vector<std::pair<int, DpgBTerm>> sterms; // (side, term): separable boundary terms
+  auto separable = [&](int a, int op) {
+    const int sp = g.test[a].space;
+    return (sp == DPG_SPACE_HGRAD && op == DPG_OP_VALUE) || (sp == DPG_SPACE_HDIV && op == DPG_OP_DOT_NORMAL);
+  };
   auto test_op_ok = [&](int a, int op, bool side) {
     if (phys_slot(a, op) >= 0) return true;
     return side && g.test[a].space == DPG_SPACE_HDIV && op == DPG_OP_DOT_NORMAL;
@@ -645,7 +650,8 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       t.kind = tr.kind;
       if (tr.kind == DPG_VAR_FIELD) { t.col0 = tr.dev_off + comp * tr.card_comp; t.ncol = tr.card_comp; }
       else { t.col0 = tr.dev_off + sg * tr.per_side; t.ncol = tr.per_side; }
-      terms.push_back({B.boundary ? 1 + sg : 0, t});
+      if (B.boundary && separable(B.test_var, B.test_op)) sterms.push_back({sg, t});
+      else terms.push_back({B.boundary ? 1 + sg : 0, t});
     }
   }
   for (int e = 0; e < D->n_rhs; e++) {
@@ -729,13 +735,15 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     S.ustride = off;
     S.rec_len = (tv + 1) & ~1;
     S.tile0 = (int)btiles.size();
+    // 16x8 blocks (row-tile pairs of the block's test var) of the active (var, column tile) blocks
     for (int kb = 0; kb < S.nblk; kb++) {
       const DpgTestVar& V = g.test[S.blk[kb].var];
-      for (int I = V.ntile0; I < V.ntile0 + V.ntiles; I++) btiles.push_back(make_int4(I, S.blk[kb].J, kb, 0));
+      for (int I = V.ntile0; I < V.ntile0 + V.ntiles; I += 2) btiles.push_back(make_int4(I, S.blk[kb].J, kb, 0));
     }
     S.ntile = (int)btiles.size() - S.tile0;
     if ((S.ntile + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_BTW)
-      return fail(DPG_ERR_UNSUPPORTED, "too many active B tiles in a segment");
+      return fail(DPG_ERR_UNSUPPORTED, "too many active B blocks in a segment");
+    if (S.nterm == 0) continue;
     g.max_rec = std::max(g.max_rec, S.rec_len);
     g.max_ustride = std::max(g.max_ustride, S.ustride);
     g.max_nterm = std::max(g.max_nterm, S.nterm);
@@ -751,24 +759,26 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   // chunk size: all points of a side in one chunk when it fits; the volume in equal chunks
   {
     auto fits = [&](int ch) {
-      int need = 2 * ch * g.max_rec + ch * g.max_ustride + g.nbpts * 24 + ch * g.max_nterm * 4 +
-                 g.nslots * g.Ptot + 64;
+      int need = 2 * ch * g.max_rec + ch * g.max_ustride + g.nbpts * 24 + g.nslots * g.Ptot + 64 +
+                 (int)sterms.size() * g.QS + 16;
       return need <= budget;
     };
-    int ch = std::min(DPG_MAX_CHB, std::max(g.QS, 1));
-    while (ch > 1 && !fits(ch)) ch--;
+    // chunks are multiples of 4 points (one m16n8k16 k-step = 4 points x 4 slots)
+    int ch = DPG_MAX_CHB;
+    while (ch > 4 && !fits(ch)) ch -= 4;
     if (!fits(ch)) return fail(DPG_ERR_UNSUPPORTED, "B-phase staging does not fit in shared memory");
     for (int sg = 0; sg < g.nseg; sg++) {
       DpgSeg& S = g.seg[sg];
-      int nch = (S.npts + ch - 1) / ch;
-      S.nchunk = nch;
-      S.chunk = (S.npts + nch - 1) / nch;  // balanced chunks
+      if (S.nterm == 0) continue;
+      S.chunk = std::min(ch, (S.npts + 3) & ~3);
+      S.nchunk = (S.npts + S.chunk - 1) / S.chunk;  // the last chunk may be short
       g.max_chunk = std::max(g.max_chunk, S.chunk);
     }
   }
   // per-segment point records: reference slots of every test var, then each term's trial values
   for (int sg = 0; sg < g.nseg; sg++) {
     DpgSeg& S = g.seg[sg];
+    if (S.nterm == 0) continue;
     const int npad = S.nchunk * S.chunk;
     std::vector<double> xs((size_t)npad * d, 0.0);
     for (int q = 0; q < npad; q++) {
@@ -800,6 +810,101 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     S.rec = upload(P, rec);
   }
 
+  // separable side terms -> entries (row, col) with per-point weights
+  if (sterms.size() > 0) {
+    std::vector<double> sidex((size_t)g.QS * d);
+    std::vector<DpgSideTerm> ses;
+    std::map<std::pair<int, int>, std::vector<std::pair<int, std::vector<double>>>> ent;  // (row, col) -> (se, W[q])
+    for (size_t e = 0; e < sterms.size(); e++) {
+      const int sd = sterms[e].first;
+      const DpgBTerm& t = sterms[e].second;
+      const DpgTestVar& V = g.test[t.test_var];
+      const bool normal_trace = V.space == DPG_SPACE_HDIV && t.test_op == DPG_OP_DOT_NORMAL;
+      DpgSideTerm st;
+      st.side = sd;
+      st.pbase = g.QG + g.QB + sd * g.QS;
+      st.slot = t.slot;
+      st.normal_comp = t.normal_comp;
+      st.flux = t.kind == DPG_VAR_FLUX;
+      st.use_meas = normal_trace ? 0 : 1;
+      st.coef = t.coef;
+      const int se = (int)ses.size();
+      ses.push_back(st);
+      for (int q = 0; q < g.QS; q++)
+        for (int k = 0; k < d; k++) sidex[(size_t)q * d + k] = sidepts[((size_t)sd * g.QSpad + q) * d + k];
+      std::vector<double> sl = fref_table(sidex.data(), g.QS);
+      // reference side values of the test operator: T[q][r]
+      std::vector<double> T((size_t)g.QS * V.card, 0.0);
+      double tmax = 0.0;
+      for (int q = 0; q < g.QS; q++) {
+        const double* f = &sl[(size_t)q * g.featstride + V.foff];
+        double c[3] = {0.0, 0.0, 0.0};
+        if (normal_trace) {
+          const double* tq = &sideT[((size_t)sd * g.QSpad + q) * 6];
+          if (d == 2) { c[0] = tq[1]; c[1] = -tq[0]; }
+          else {
+            c[0] = tq[1] * tq[5] - tq[2] * tq[4];
+            c[1] = tq[2] * tq[3] - tq[0] * tq[5];
+            c[2] = tq[0] * tq[4] - tq[1] * tq[3];
+          }
+        }
+        for (int r = 0; r < V.card; r++) {
+          double v;
+          if (normal_trace) {
+            v = 0.0;
+            for (int k = 0; k < d; k++) v += c[k] * f[k * V.ldA + r];
+            v *= rS.w[q];
+          } else {
+            v = f[r];
+          }
+          T[(size_t)q * V.card + r] = v;
+          tmax = std::max(tmax, std::fabs(v));
+        }
+      }
+      const DpgTrialVar& tr = g.trial[t.trial_var];
+      for (int r = 0; r < V.card; r++) {
+        double rmax = 0.0;
+        for (int q = 0; q < g.QS; q++) rmax = std::max(rmax, std::fabs(T[(size_t)q * V.card + r]));
+        if (!(rmax > 1e-14 * tmax)) continue;  // zero on this side (to roundoff)
+        for (int m = 0; m < t.ncol; m++) {
+          std::vector<double> W(g.QS);
+          for (int q = 0; q < g.QS; q++) {
+            double tv = (t.kind == DPG_VAR_FIELD) ? host_tabS[t.trial_var][((size_t)sd * g.QSpad + q) * tr.card_comp + m]
+                                                  : host_tabS[t.trial_var][(size_t)q * tr.per_side + m];
+            W[q] = T[(size_t)q * V.card + r] * tv;
+          }
+          ent[{V.dev_off + r, t.col0 + m}].push_back({se, W});
+        }
+      }
+    }
+    std::vector<int4> sent;
+    std::vector<int> scon_se;
+    std::vector<std::vector<double>> wl;
+    for (auto& kv : ent) {
+      sent.push_back(make_int4(kv.first.first, kv.first.second, (int)scon_se.size(), (int)kv.second.size()));
+      for (auto& c : kv.second) { scon_se.push_back(c.first); wl.push_back(c.second); }
+    }
+    g.nse = (int)ses.size();
+    g.nsent = (int)sent.size();
+    g.ncon = (int)scon_se.size();
+    std::vector<double> wq((size_t)g.QS * g.ncon);
+    for (int c = 0; c < g.ncon; c++)
+      for (int q = 0; q < g.QS; q++) wq[(size_t)q * g.ncon + c] = wl[c][q];
+    void* p = nullptr;
+    if (cudaMalloc(&p, ses.size() * sizeof(DpgSideTerm)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
+    cudaMemcpy(p, ses.data(), ses.size() * sizeof(DpgSideTerm), cudaMemcpyHostToDevice);
+    P->allocs.push_back(p);
+    g.se = (const DpgSideTerm*)p;
+    p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(1, sent.size()) * sizeof(int4)) != cudaSuccess)
+      return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
+    if (!sent.empty()) cudaMemcpy(p, sent.data(), sent.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    P->allocs.push_back(p);
+    g.sent = (const int4*)p;
+    g.scon_se = upload_i(P, scon_se);
+    g.scon_w = upload(P, wq);
+  }
+
   // ---- shared memory layout (doubles) ----------------------------------------
   {
     auto al = [](int x) { return (x + 15) & ~15; };  // 128-byte aligned regions
@@ -825,7 +930,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     g.b_rec1 = o; o += al(g.max_chunk * g.max_rec);
     g.b_u = o; o += al(g.max_chunk * g.max_ustride);
     g.b_geo = o; o += al(g.nbpts * 24);
-    g.b_R = o; o += al(g.max_chunk * g.max_nterm * 4);
+    g.b_fac = o; o += al(g.nse * g.QS);
     int bphase = o;
     g.sm_w = 0;
     int wsz = g.MBT * g.NBT * 64;

@@ -60,6 +60,15 @@ __device__ __forceinline__ void dmma16(double* c, const double* a, const double*
         "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
+// D(16x8) += A(16x8) * B(8x8): a0 = A[g][t], a1 = A[g+8][t], a2 = A[g][t+4], a3 = A[g+8][t+4];
+// b0 = B[t][g], b1 = B[t+4][g]; c_lo holds rows g, c_hi rows g+8 (columns 2t, 2t+1 each).
+__device__ __forceinline__ void dmma16x8(double2& c_lo, double2& c_hi, double a0, double a1, double a2, double a3,
+                                         double b0, double b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(c_lo.x), "+d"(c_lo.y), "+d"(c_hi.x), "+d"(c_hi.y)
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
@@ -387,14 +396,13 @@ __device__ __noinline__ void tile_cholesky(int T_off, int nb, int nsteps, int fl
 // Phase 1: B and F -> per-CTA scratch (or the B/F outputs in parts mode)
 // ---------------------------------------------------------------------------
 template <int BTW>
-__device__ __forceinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+__device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int d = P.d, nv = P.nv;
   DPG_SMEM_VIEWS(P);
   double* geo = sm + P.b_geo;
   double* U = sm + P.b_u;
-  double* R = sm + P.b_R;
   const int8_t* par_c = L.parity + (size_t)cell * P.ns;
   double2* scr = reinterpret_cast<double2*>(L.scratch + (size_t)blockIdx.x * P.scratch_per_cta);
   // prologue: first chunk's records in flight while the geometry is computed
@@ -402,7 +410,7 @@ __device__ __forceinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L,
   while (first_seg < P.nseg && P.seg[first_seg].nterm == 0) first_seg++;
   if (tid == 0 && first_seg < P.nseg) {
     const DpgSeg& S = P.seg[first_seg];
-    const uint32_t bytes = (uint32_t)(S.chunk * S.rec_len * sizeof(double));
+    const uint32_t bytes = (uint32_t)(((min(S.chunk, S.npts) + 3) & ~3) * S.rec_len * sizeof(double));
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&mbar_s[2], bytes);
     bulk_g2s(sm + P.b_rec0, S.rec, bytes, &mbar_s[2]);
@@ -416,28 +424,28 @@ __device__ __forceinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L,
   for (int sgi = first_seg; sgi < P.nseg; sgi++) {
     const DpgSeg& S = P.seg[sgi];
     if (S.nterm == 0) continue;
-    // this warp's active tiles of the segment: operand offsets and accumulators
+    // this warp's active 16x8 blocks of the segment: operand offsets and accumulators
     const int per = (S.ntile + DPG_NWARPS - 1) / DPG_NWARPS;
     const int my0 = S.tile0 + warp * per;
     const int nmine = max(0, min(per, S.tile0 + S.ntile - my0));
-    int aoff[BTW], boff[BTW];
-    double2 acc[BTW];
+    uint32_t pk[BTW];
+    double acc[BTW][4];
 #pragma unroll
     for (int u = 0; u < BTW; u++) {
-      acc[u] = make_double2(0.0, 0.0);
-      aoff[u] = 0; boff[u] = 0;
+      acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+      uint32_t v = 0;
       if (u < nmine) {
         const int4 td = P.btiles[my0 + u];
         const DpgBBlock& Bk = S.blk[td.z];
         const DpgTestVar& V = P.test[Bk.var];
-        aoff[u] = V.foff + t * V.ldA + (td.x - V.ntile0) * 8 + g;
-        boff[u] = Bk.off + t * DPG_ULD + g;
+        v = (uint32_t)(V.foff + t * V.ldA + (td.x - V.ntile0) * 8 + g) | ((uint32_t)(Bk.off + t * DPG_ULD + g) << 16);
       }
+      pk[u] = v;
     }
     for (int c = 0; c < S.nchunk; c++, gc++) {
       const int buf = gc & 1;
       double* rec = sm + (buf ? P.b_rec1 : P.b_rec0);
-      __syncthreads();  // the other buffer, U and R are free; geometry is complete
+      __syncthreads();  // the other buffer and U are free; geometry is complete
       if (tid == 0) {
         // prefetch the next chunk (this segment or the next one with terms)
         int ns = sgi, nc = c + 1;
@@ -448,79 +456,121 @@ __device__ __forceinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L,
         }
         if (ns < P.nseg) {
           const DpgSeg& S2 = P.seg[ns];
-          const uint32_t bytes = (uint32_t)(S2.chunk * S2.rec_len * sizeof(double));
+          // the records of the chunk's points, rounded up to a whole k-step (the table is padded)
+          const uint32_t bytes =
+              (uint32_t)(((min(S2.chunk, S2.npts - nc * S2.chunk) + 3) & ~3) * S2.rec_len * sizeof(double));
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           mbar_expect_tx(&mbar_s[2 + (buf ^ 1)], bytes);
           bulk_g2s(sm + (buf ? P.b_rec0 : P.b_rec1), S2.rec + (size_t)nc * S2.chunk * S2.rec_len, bytes,
                    &mbar_s[2 + (buf ^ 1)]);
         }
-      }
-      const int q0 = c * S.chunk;
-      const int nq = min(S.chunk, S.npts - q0);
-      // term rows R[lq][lt][4] = w*|J| * coef * slot * (n) * (parity) * T_op
-      for (int task = tid; task < S.chunk * S.nterm; task += NT) {
-        const int lq = task / S.nterm, lt = task - lq * S.nterm;
-        double* r = R + task * 4;
-        if (lq >= nq) { r[0] = r[1] = r[2] = r[3] = 0.0; continue; }
-        const int q = q0 + lq;
-        const DpgBTerm& Tm = P.bterm[S.term0 + lt];
-        const double* gq = geo + (S.geo0 + q) * GEO;
-        double v = gq[19] * Tm.coef;
-        if (Tm.slot >= 0) v *= coef_s[Tm.slot * P.Ptot + S.pbase + q];
-        if (Tm.normal_comp >= 0) v *= gq[20 + Tm.normal_comp];
-        if (Tm.kind == DPG_VAR_FLUX) v *= (double)par_c[S.side];
-        double tr[4];
-        trow_op(P.test[Tm.test_var].space, d, Tm.test_op, gq, tr);
-        r[0] = v * tr[0]; r[1] = v * tr[1]; r[2] = v * tr[2]; r[3] = v * tr[3];
-      }
-      if (tid == 0) {
         if (!mbar_wait(&mbar_s[2 + buf], X.phase[2 + buf] & 1)) flag_s[2] = 1;
       }
       X.phase[2 + buf]++;
+      const int q0 = c * S.chunk;
+      const int nq = min(S.chunk, S.npts - q0);
       __syncthreads();
-      // U blocks: U[lq][blk][m][col] = sum over the block's terms of R[lq][lt][m] * trial value
+      // U blocks: U[lq][blk][m][col] = sum over the block's terms of
+      //   (w*|J| * coef * slot * (n) * (parity) * T_op[m]) * trial value
       for (int task = tid; task < S.chunk * S.nblk * 8; task += NT) {
         const int lq = task / (S.nblk * 8);
         const int rem = task - lq * S.nblk * 8;
         const int kb = rem >> 3, cl = rem & 7;
         const DpgBBlock& Bk = S.blk[kb];
         const int col = Bk.J * 8 + cl;
-        const double* rq = rec + lq * S.rec_len;
         double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
-        for (int i = 0; i < Bk.nt; i++) {
-          const int lt = Bk.terms[i];
-          const DpgBTerm& Tm = P.bterm[S.term0 + lt];
-          const int mm = col - Tm.col0;
-          if (mm < 0 || mm >= Tm.ncol) continue;
-          const double val = rq[S.tvoff[lt] + mm];
-          const double* r = R + (lq * S.nterm + lt) * 4;
-          u0 += r[0] * val; u1 += r[1] * val; u2 += r[2] * val; u3 += r[3] * val;
+        if (lq < nq) {
+          const int q = q0 + lq;
+          const double* rq = rec + lq * S.rec_len;
+          const double* gq = geo + (S.geo0 + q) * GEO;
+          const int space = P.test[Bk.var].space;
+          for (int i = 0; i < Bk.nt; i++) {
+            const int lt = Bk.terms[i];
+            const DpgBTerm& Tm = P.bterm[S.term0 + lt];
+            const int mm = col - Tm.col0;
+            if (mm < 0 || mm >= Tm.ncol) continue;
+            double v = gq[19] * Tm.coef * rq[S.tvoff[lt] + mm];
+            if (Tm.slot >= 0) v *= coef_s[Tm.slot * P.Ptot + S.pbase + q];
+            if (Tm.normal_comp >= 0) v *= gq[20 + Tm.normal_comp];
+            if (Tm.kind == DPG_VAR_FLUX) v *= (double)par_c[S.side];
+            double tr[4];
+            trow_op(space, d, Tm.test_op, gq, tr);
+            u0 += tr[0] * v; u1 += tr[1] * v; u2 += tr[2] * v; u3 += tr[3] * v;
+          }
         }
         double* uq = U + lq * S.ustride + Bk.off + cl;
         uq[0] = u0; uq[DPG_ULD] = u1; uq[2 * DPG_ULD] = u2; uq[3 * DPG_ULD] = u3;
       }
       __syncthreads();
-      // DMMA over this warp's active tiles of the segment: one k-step (4 slots) per point
+      // DMMA over this warp's active blocks of the segment: m16n8k16, one k-step = 4 points x 4 slots
 #pragma unroll 1
-      for (int lq = 0; lq < nq; lq++) {
-        const double* ra = rec + lq * S.rec_len;
-        const double* ub = U + lq * S.ustride;
+      for (int s4 = 0; s4 < nq; s4 += 4) {
+        const double* ra = rec + s4 * S.rec_len;
+        const double* ub = U + s4 * S.ustride;
+        uint32_t prevA = 0xffffffffu;
+        double av[8];
 #pragma unroll
-        for (int u = 0; u < BTW; u++)
-          if (u < nmine) dmma(acc[u], ra[aoff[u]], ub[boff[u]]);
+        for (int u = 0; u < BTW; u++) {
+          if (u < nmine) {
+            const uint32_t ao = pk[u] & 0xffffu, bo = pk[u] >> 16;
+            if (ao != prevA) {
+#pragma unroll
+              for (int i = 0; i < 4; i++) {
+                av[2 * i] = ra[i * S.rec_len + ao];
+                av[2 * i + 1] = ra[i * S.rec_len + ao + 8];
+              }
+              prevA = ao;
+            }
+            double bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) bv[i] = ub[i * S.ustride + bo];
+            dmma16(acc[u], av, bv);
+          }
+        }
       }
     }
-    // segment contributions into the scratch tiles (each tile has one owner per segment)
+    // segment contributions into the scratch tiles (each block has one owner per segment)
 #pragma unroll
     for (int u = 0; u < BTW; u++) {
       if (u < nmine) {
         const int4 td = P.btiles[my0 + u];
-        const int si = (td.y * P.NBT + td.x) * 32 + lane;
-        double2 v = scr[si];
-        v.x += acc[u].x;
-        v.y += acc[u].y;
-        scr[si] = v;
+        const int s0 = (td.y * P.NBT + td.x) * 32 + lane;
+        double2 v0 = scr[s0], v1 = scr[s0 + 32];
+        v0.x += acc[u][0]; v0.y += acc[u][1];
+        v1.x += acc[u][2]; v1.y += acc[u][3];
+        scr[s0] = v0;
+        scr[s0 + 32] = v1;
       }
+    }
+  }
+  // separable side terms: one thread per entry (row, col); entries are unique, so the
+  // read-modify-write of the scratch element needs no atomics
+  if (P.nse > 0) {
+    double* fac = sm + P.b_fac;  // [nse][QS]
+    __syncthreads();             // segment contributions are in the scratch
+    for (int task = tid; task < P.nse * P.QS; task += NT) {
+      const int se = task / P.QS, q = task - se * P.QS;
+      const DpgSideTerm& E = P.se[se];
+      const double* gq = geo + (P.QB + E.side * P.QS + q) * GEO;
+      double v = E.coef;
+      if (E.use_meas) v *= gq[19];
+      if (E.slot >= 0) v *= coef_s[E.slot * P.Ptot + E.pbase + q];
+      if (E.normal_comp >= 0) v *= gq[20 + E.normal_comp];
+      if (E.flux) v *= (double)par_c[E.side];
+      fac[task] = v;
+    }
+    __syncthreads();
+    double* scd = reinterpret_cast<double*>(scr);
+    for (int e = tid; e < P.nsent; e += NT) {
+      const int4 en = __ldg(P.sent + e);
+      double acc = 0.0;
+      for (int c = en.z; c < en.z + en.w; c++) {
+        const double* f = fac + __ldg(P.scon_se + c) * P.QS;
+        for (int q = 0; q < P.QS; q++) acc += __ldg(P.scon_w + (size_t)q * P.ncon + c) * f[q];
+      }
+      const int r = en.x & 7, cc = en.y & 7;
+      const size_t idx = ((size_t)((en.y >> 3) * P.NBT + (en.x >> 3)) * 32 + r * 4 + (cc >> 1)) * 2 + (cc & 1);
+      scd[idx] += acc;
     }
   }
   if (!L.parts) return;
@@ -760,7 +810,7 @@ __device__ __forceinline__ void phase_factor(const DpgPlanDev& P, const Ctx& X) 
 // Phase 4: W = L^-1 [B | F] per column tile in registers, W^T tiles to smem
 // ---------------------------------------------------------------------------
 template <int NBTM>
-__device__ __noinline__ void phase_trsm(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
+__device__ __forceinline__ void phase_trsm(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   DPG_SMEM_VIEWS(P);
@@ -814,10 +864,14 @@ __device__ __noinline__ void phase_trsm(const DpgPlanDev& P, const DpgLaunch& L,
         cfrag_to_bfrag(x, lane, x0, x1);
         x0 = -x0;
         x1 = -x1;
+        // rows i, i+1 together: one m16n8k8 on the stacked tiles [L_ik; L_i+1,k]
 #pragma unroll
-        for (int i = k + 1; i < NBTM; i++) {
-          if (i < P.NBT) {
-            const double* Lik = GT + (i * (i + 1) / 2 + k) * 64;
+        for (int i = k + 1; i < NBTM; i += 2) {
+          const double* Lik = GT + (i * (i + 1) / 2 + k) * 64;
+          if (i + 1 < NBTM && i + 1 < P.NBT) {
+            const double* Li1k = GT + ((i + 1) * (i + 2) / 2 + k) * 64;
+            dmma16x8(bacc[i], bacc[i + 1], Lik[lane], Li1k[lane], Lik[32 + lane], Li1k[32 + lane], x0, x1);
+          } else if (i < P.NBT) {
             dmma(bacc[i], Lik[lane], x0);
             dmma(bacc[i], Lik[32 + lane], x1);
           }
@@ -1006,7 +1060,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
 
 // Instances: register arrays sized for the test-tile count of the bucket.
 #define DPG_INSTANCES(X) \
-  X(8, 3, 8) X(12, 5, 8) X(16, 6, 8) X(18, 8, 8) X(20, 8, 8) X(22, 9, 8) X(24, 12, 8) X(24, 12, 12)
+  X(8, 3, 4) X(12, 5, 4) X(16, 6, 4) X(18, 8, 4) X(20, 8, 4) X(22, 9, 3) X(24, 12, 4) X(24, 12, 6)
 
 typedef void (*KernelFn)(const DpgPlanDev, const DpgLaunch);
 

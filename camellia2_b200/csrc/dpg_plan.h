@@ -56,6 +56,21 @@ struct DpgBTerm {
   int col0, ncol; // device trial columns touched (contiguous)
 };
 
+// A boundary term whose test operator has a cell-independent side transform
+// (HGRAD value; HDIV normal trace through the Piola identity
+// (J v / det J) . n |J_s| = v . (t_0 x t_1) on the reference side), on one side.
+// Per point it contributes factor(q) * W[q][c] to each of its entries c, with the
+// cell-independent weights W = reference test value x trial value.
+struct DpgSideTerm {
+  int side;
+  int pbase;        // first coefficient point of the side
+  int slot;         // coefficient slot or -1
+  int normal_comp;  // multiply by n_c, or -1
+  int flux;         // multiply by the side parity
+  int use_meas;     // 1: factor w |J_s| from the geometry; 0: the side weight is inside W
+  double coef;
+};
+
 struct DpgBBlock {
   int var;        // test var
   int J;          // trial column tile
@@ -147,6 +162,13 @@ struct DpgPlanDev {
   const double* tangB;      // [nbpts][6] reference side tangents (zero for volume points)
   int max_rec, max_chunk, max_ustride, max_nterm;
   const int4* btiles;       // active B tiles of all segments: (I, J, block, 0)
+  // separable side terms: B[row][col] += sum_c sum_q W[q][c] factor_se(c)(q) over the
+  // contributions c of each entry (row, col)
+  int nse, nsent, ncon;
+  const DpgSideTerm* se;    // [nse]
+  const int4* sent;         // [nsent] (device row, device column, first contribution, count)
+  const int* scon_se;       // [ncon] side term of each contribution
+  const double* scon_w;     // [QS][ncon]
   // index maps
   const int* dev2user_trial;  // [Mp] -> user trial index, or -1
   const int* dev2user_test;   // [Np] -> user test index, or -1
@@ -157,7 +179,7 @@ struct DpgPlanDev {
   int sm_coef;    // per cell: coefficients [nslots][Ptot]
   int g_fref0, g_fref1, g_h, g_geo, g_D, g_beta;   // Gram phase (g_beta overlaps g_h)
   int sm_gt, sm_linv, sm_scale, sm_invd;           // factor
-  int b_rec0, b_rec1, b_u, b_geo, b_R;             // B phase
+  int b_rec0, b_rec1, b_u, b_geo, b_fac;      // B phase
   int sm_w, sm_k;                                  // solve / Gram of W
   size_t scratch_per_cta;                          // doubles of B scratch per CTA
 };
