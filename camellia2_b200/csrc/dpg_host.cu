@@ -23,6 +23,8 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+
+#define DPG_CHA_HOST 4  // points per reverse-mode pull-back chunk (DPG_CHA in the kernel)
 #include <string>
 #include <vector>
 
@@ -903,7 +905,38 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     g.sent = (const int4*)p;
     g.scon_se = upload_i(P, scon_se);
     g.scon_w = upload(P, wq);
+    // reverse mode: contributions grouped by side term, with their (row, col)
+    std::vector<int> sstart(g.nse + 1, 0), scon;
+    std::vector<int2> rc(g.ncon);
+    for (size_t e = 0; e < sent.size(); e++)
+      for (int c = sent[e].z; c < sent[e].z + sent[e].w; c++) rc[c] = make_int2(sent[e].x, sent[e].y);
+    for (int se = 0; se < g.nse; se++) {
+      sstart[se] = (int)scon.size();
+      for (int c = 0; c < g.ncon; c++)
+        if (scon_se[c] == se) scon.push_back(c);
+    }
+    sstart[g.nse] = (int)scon.size();
+    g.sadj_start = upload_i(P, sstart);
+    g.sadj_con = upload_i(P, scon);
+    p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(1, rc.size()) * sizeof(int2)) != cudaSuccess)
+      return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
+    if (!rc.empty()) cudaMemcpy(p, rc.data(), rc.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    P->allocs.push_back(p);
+    g.scon_rc = (const int2*)p;
+    for (const DpgSideTerm& st : ses) g.se_slots |= st.slot >= 0;
   }
+  // coefficient uses the reverse mode covers: IP entries, volume B and load terms,
+  // separable side terms
+  for (int e = 0; e < g.nipent; e++) g.ip_slots |= g.ipent[e].slot >= 0;
+  bool adj_terms_ok = true;
+  for (int sg = 0; sg < g.nseg; sg++)
+    for (int lt = 0; lt < g.seg[sg].nterm; lt++) {
+      const DpgBTerm& t = g.bterm[g.seg[sg].term0 + lt];
+      if (t.slot < 0) continue;
+      if (sg == 0) g.b_slots = 1;
+      else adj_terms_ok = false;  // a non-separable side term with a coefficient
+    }
 
   // ---- shared memory layout (doubles) ----------------------------------------
   {
@@ -939,6 +972,23 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     if (g.sm_linv < ksz || g.sm_linv + g.MBT * 64 > g.sm_linv + al(g.NBT * 64))
       return fail(DPG_ERR_UNSUPPORTED, "trial tiles outnumber test tiles: condensation workspace overlaps K");
     int body = std::max(std::max(gphase, bphase), std::max(std::max(wsz, ksz), fphase));
+    // reverse mode: S_A, then the pull-back staging (both reuse the body after the factor)
+    {
+      const int Mx = g.MBT * 8;
+      g.a_ldS = ((Mx + 15) & ~15) + 4;  // == 4 mod 16: conflict-free B-fragments
+      g.a_sa = 0;
+      const int sa_end = Mx * g.a_ldS;
+      int fsl = g.featstride;
+      if (g.seg[0].nterm > 0) fsl = std::max(fsl, g.seg[0].rec_len);
+      int q = 0;
+      g.a_fs = q; q += al(DPG_CHA_HOST * fsl);
+      g.a_ldx = 2 * Mx;
+      g.a_xpf = q; q += al(DPG_CHA_HOST * g.ntest * 4 * g.a_ldx);
+      g.a_geo = q; q += al(std::max(DPG_CHA_HOST, g.ns * g.QS) * 24);
+      g.a_beta = q; q += al(DPG_CHA_HOST * g.niprows * 4 * g.ntest);
+      g.a_cbar = q; q += al(std::max(1, g.nslots * g.Ptot));
+      g.adj_ok = adj_terms_ok && std::max(sa_end, q) <= body && g.QB > 0;
+    }
     g.sm_coef = al(body);
     g.sm_tiles = g.sm_coef + al(std::max(1, g.nslots * g.Ptot));
     g.sm_nodes = g.sm_tiles + al((g.ngb * (int)sizeof(DpgGTile) + 7) / 8);
@@ -1218,9 +1268,20 @@ int dpg_factored_cholesky_solve(int C, int N, int M, const double* G, const doub
 
 int dpg_assemble_adjoint(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff,
                          const double* Kbar, const double* lbar, double* coeff_bar, int32_t* info, void* stream) {
-  (void)p; (void)C; (void)nodes; (void)parity; (void)coeff; (void)Kbar; (void)lbar; (void)coeff_bar; (void)info;
-  (void)stream;
-  return fail(DPG_ERR_UNSUPPORTED, "adjoint not built yet");
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!nodes || !parity || !info || !Kbar) return fail(DPG_ERR_INVALID_ARGUMENT, "nodes, parity, Kbar and info are required");
+  const DpgPlanDev& g = p->hp.dev;
+  if (g.nslots > 0 && (!coeff || !coeff_bar))
+    return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients and their gradient buffer are required by this plan");
+  if (g.nslots == 0) return DPG_OK;  // nothing to differentiate
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.nodes = nodes; L.parity = parity; L.coeff = coeff;
+  L.info = info;
+  L.Kbar = Kbar; L.lbar = lbar; L.coeff_bar = coeff_bar;
+  return dpg_launch_adjoint(&g, &L, (cudaStream_t)stream);
 }
 
 int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags) {

@@ -34,6 +34,11 @@ struct DpgLaunch {
   const double* Fin;
   // B tiles between the B phase and the triangular solve: scratch_per_cta doubles per CTA
   double* scratch;
+  // dpg_assemble_adjoint: loss gradients in, coefficient gradients out; scratch2 holds P
+  const double* Kbar;
+  const double* lbar;
+  double* coeff_bar;
+  double* scratch2;
 };
 
 int dpg_configure_kernels(const DpgPlanDev* plan);
@@ -43,3 +48,4 @@ int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d
                       double* K, double* l, double* S, double* s, int32_t* info, int flags);
 int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
+int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);

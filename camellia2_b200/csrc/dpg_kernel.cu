@@ -1075,6 +1075,8 @@ static KernelFn pick_kernel(const DpgPlanDev* plan) {
   return nullptr;
 }
 
+#include "dpg_adjoint.cuh"
+
 static int g_num_sms = 0;
 
 }  // namespace
@@ -1085,6 +1087,14 @@ int dpg_configure_kernels(const DpgPlanDev* plan) {
   size_t bytes = (size_t)plan->sm_total * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  if (plan->adj_ok) {
+    KernelFn ka = pick_adjoint_kernel(plan);
+    if (ka) {
+      e = cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      if (e != cudaSuccess)
+        return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    }
+  }
   if (g_num_sms == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1122,6 +1132,30 @@ int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const 
   k<<<grid, NT, bytes, stream>>>(*plan, L);
   cudaError_t e = cudaGetLastError();
   if (scratch) cudaFreeAsync(scratch, stream);
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
+int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
+  if (Lin->C <= 0) return DPG_OK;
+  if (!plan->adj_ok) return dpg::fail(DPG_ERR_UNSUPPORTED, "reverse mode is not available for this bucket");
+  KernelFn k = pick_adjoint_kernel(plan);
+  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no adjoint kernel instance for this bucket size");
+  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  DpgLaunch L = *Lin;
+  void* scratch = nullptr;
+  const size_t per = plan->scratch_per_cta;
+  cudaError_t ea = cudaMallocAsync(&scratch, (size_t)grid * per * 2 * sizeof(double), stream);
+  if (ea != cudaSuccess) {
+    cudaGetLastError();
+    return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(ea));
+  }
+  L.scratch = (double*)scratch;
+  L.scratch2 = L.scratch + (size_t)grid * per;
+  size_t bytes = (size_t)plan->sm_total * sizeof(double);
+  k<<<grid, NT, bytes, stream>>>(*plan, L);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(scratch, stream);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
 }

@@ -169,6 +169,12 @@ struct DpgPlanDev {
   const int4* sent;         // [nsent] (device row, device column, first contribution, count)
   const int* scon_se;       // [ncon] side term of each contribution
   const double* scon_w;     // [QS][ncon]
+  // reverse mode (dpg_assemble_adjoint)
+  int adj_ok;               // the adjoint's workspaces fit and every coefficient use is supported
+  int ip_slots, b_slots, se_slots;  // coefficient slots occur in the IP / volume B and load / side terms
+  const int* sadj_start;    // [nse + 1] contributions of each side term
+  const int* sadj_con;      // contribution indices grouped by side term
+  const int2* scon_rc;      // [ncon] (device row, device column) of each contribution
   // index maps
   const int* dev2user_trial;  // [Mp] -> user trial index, or -1
   const int* dev2user_test;   // [Np] -> user test index, or -1
@@ -181,5 +187,7 @@ struct DpgPlanDev {
   int sm_gt, sm_linv, sm_scale, sm_invd;           // factor
   int b_rec0, b_rec1, b_u, b_geo, b_fac;      // B phase
   int sm_w, sm_k;                                  // solve / Gram of W
+  int a_sa, a_ldS;                                 // adjoint: S_A [MBT*8][a_ldS]
+  int a_fs, a_xpf, a_ldx, a_geo, a_beta, a_cbar;   // adjoint pull-back
   size_t scratch_per_cta;                          // doubles of B scratch per CTA
 };

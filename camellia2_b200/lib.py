@@ -140,6 +140,19 @@ class Plan:
                                          _ptr(F), _stream_ptr(stream)))
         return G, B, F
 
+    def adjoint(self, nodes, parity, coeff, Kbar, lbar=None, stream=None):
+        """dJ/dcoeff (C, n_slots, n_points_total) for a loss J(K, l) with Kbar = dJ/dK (C,M,M)
+        and lbar = dJ/dl (C,M); device tensors (dpg_assemble_adjoint)."""
+        import torch
+        C = nodes.shape[0]
+        i = self.info
+        cbar = torch.zeros((C, i["n_slots"], i["n_points_total"]), dtype=torch.float64, device=nodes.device)
+        info = torch.empty((C,), dtype=torch.int32, device=nodes.device)
+        _check(load().dpg_assemble_adjoint(self.h, C, _ptr(nodes), _ptr(parity), _ptr(coeff),
+                                           _ptr(Kbar.contiguous()), _ptr(None if lbar is None else lbar.contiguous()),
+                                           _ptr(cbar), _ptr(info), _stream_ptr(stream)))
+        return cbar, info
+
     # -------------------------------------------------------------------- host
     def assemble_host(self, nodes, parity, coeff=None, out=None, flags=0):
         """Host arrays (numpy or CPU torch, pinned is fastest) in and out."""

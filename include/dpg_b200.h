@@ -210,8 +210,11 @@ int dpg_factored_cholesky_solve(int C, int N, int M, const double* G, const doub
                                 void* stream);
 
 /* Adjoint of dpg_assemble (K and l outputs) for a loss J(K, l):
- * given Kbar (C,M,M) and lbar (C,M) = dJ/dK, dJ/dl, writes
- * coeff_bar (C, n_slots, n_points_total) = dJ/dcoeff. Device pointers. */
+ * given Kbar (C,M,M) and lbar (C,M) = dJ/dK, dJ/dl (lbar may be NULL), writes
+ * coeff_bar (C, n_slots, n_points_total) = dJ/dcoeff. Device pointers.
+ * Covers coefficients in the inner product, in volume bilinear and load terms
+ * and in boundary terms whose test operator is a value or a normal trace;
+ * other plans return DPG_ERR_UNSUPPORTED. No counterpart in the reference. */
 int dpg_assemble_adjoint(dpg_plan* plan, int C, const double* nodes, const int8_t* parity,
                          const double* coeff, const double* Kbar, const double* lbar,
                          double* coeff_bar, int32_t* info, void* stream);
