@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 
 #define DPG_CHA_HOST 4  // points per reverse-mode pull-back chunk (DPG_CHA in the kernel)
 #include <string>
@@ -196,22 +197,222 @@ static int card_hgrad(int dim, int p) {
 static int card_hdiv(int dim, int n) { return dim == 2 ? 2 * n * (n + 1) : 3 * n * n * (n + 1); }
 
 // ----------------------------------------------------------------------------
+// Triangle bases (Intrepid Basis_HGRAD_TRI_Cn_FEM on the warp & blend lattice,
+// Basis_HDIV_TRI_In_FEM = Raviart-Thomas RT_n; BasisFactory.cpp:198-350).  The
+// lattice follows the published warp & blend construction (Warburton 2006,
+// optimized alpha table); the Lagrange functions are built through the
+// orthonormal PKD (Dubiner) polynomials, whose Vandermonde matrix on the lattice
+// is well conditioned.  RT_n uses the modal basis (p,0), (0,p) for p in P_{n-1}
+// and x h for homogeneous h of degree n-1: only the span of a test space enters
+// K, l and S.
+// ----------------------------------------------------------------------------
+
+// Orthonormal Jacobi polynomial P_n^{(a,b)} on [-1,1].
+static double jacobi_p(double x, double a, double b, int n) {
+  const double g0 =
+      std::pow(2.0, a + b + 1) / (a + b + 1) * std::tgamma(a + 1) * std::tgamma(b + 1) / std::tgamma(a + b + 1);
+  double pm = 1.0 / std::sqrt(g0);
+  if (n == 0) return pm;
+  const double g1 = (a + 1) * (b + 1) / (a + b + 3) * g0;
+  double pc = ((a + b + 2) * x / 2 + (a - b) / 2) / std::sqrt(g1);
+  double an = 2.0 / (2 + a + b) * std::sqrt((a + 1) * (b + 1) / (a + b + 3));
+  for (int i = 1; i < n; i++) {
+    const double h = 2.0 * i + a + b;
+    const double an1 = 2.0 / (h + 2) * std::sqrt((i + 1) * (i + 1 + a + b) * (i + 1 + a) * (i + 1 + b) / (h + 1) / (h + 3));
+    const double bn1 = -(a * a - b * b) / h / (h + 2);
+    const double pn = (-an * pm + (x - bn1) * pc) / an1;
+    pm = pc;
+    pc = pn;
+    an = an1;
+  }
+  return pc;
+}
+static double jacobi_dp(double x, double a, double b, int n) {
+  return n == 0 ? 0.0 : std::sqrt(n * (n + a + b + 1)) * jacobi_p(x, a + 1, b + 1, n - 1);
+}
+
+// PKD polynomial (i, j) at (r, s) of the biunit triangle, with d/dr and d/ds.
+static void pkd(int i, int j, double r, double s, double& v, double& dr, double& ds) {
+  const double a = (std::fabs(s - 1.0) > 1e-14) ? 2.0 * (1.0 + r) / (1.0 - s) - 1.0 : -1.0, b = s;
+  const double fa = jacobi_p(a, 0, 0, i), dfa = jacobi_dp(a, 0, 0, i);
+  const double gb = jacobi_p(b, 2 * i + 1, 0, j), dgb = jacobi_dp(b, 2 * i + 1, 0, j);
+  const double hb = 0.5 * (1.0 - b), sc = std::pow(2.0, i + 0.5);
+  v = sc * fa * gb * std::pow(hb, i);
+  double er = dfa * gb, es = dfa * gb * 0.5 * (1.0 + a);
+  if (i > 0) { er *= std::pow(hb, i - 1); es *= std::pow(hb, i - 1); }
+  double t = dgb * std::pow(hb, i);
+  if (i > 0) t -= 0.5 * i * gb * std::pow(hb, i - 1);
+  es += fa * t;
+  dr = sc * er;
+  ds = sc * es;
+}
+
+// Warp & blend lattice of degree N >= 1 on (0,0),(1,0),(0,1); rows of constant eta.
+static std::vector<double> tri_lattice(int N) {
+  static const double alpopt[15] = {0.0000, 0.0000, 1.4152, 0.1001, 0.2751, 0.9800, 1.0999, 1.2832,
+                                    1.3648, 1.4773, 1.4959, 1.5743, 1.5770, 1.6223, 1.6258};
+  const double alpha = N < 16 ? alpopt[N - 1] : 5.0 / 3.0;
+  const std::vector<double> gll = gll_nodes(N);
+  auto warp = [&](double r) {
+    double w = 0.0;
+    for (int i = 0; i <= N; i++) {
+      const double ei = -1.0 + 2.0 * i / N;
+      double l = 1.0;
+      for (int j = 0; j <= N; j++)
+        if (j != i) {
+          const double ej = -1.0 + 2.0 * j / N;
+          l *= (r - ej) / (ei - ej);
+        }
+      w += (gll[i] - ei) * l;
+    }
+    return std::fabs(r) < 1.0 - 1e-10 ? w / (1.0 - r * r) : 0.0;
+  };
+  const double s3 = std::sqrt(3.0);
+  std::vector<double> out;
+  for (int n = 0; n <= N; n++)
+    for (int m = 0; m <= N - n; m++) {
+      const double L1 = (double)n / N, L3 = (double)m / N, L2 = 1.0 - L1 - L3;
+      double x = -L2 + L3, y = (-L2 - L3 + 2 * L1) / s3;
+      const double w1 = 4 * L2 * L3 * warp(L3 - L2) * (1 + (alpha * L1) * (alpha * L1));
+      const double w2 = 4 * L1 * L3 * warp(L1 - L3) * (1 + (alpha * L2) * (alpha * L2));
+      const double w3 = 4 * L1 * L2 * warp(L2 - L1) * (1 + (alpha * L3) * (alpha * L3));
+      x += w1 + std::cos(2 * M_PI / 3) * w2 + std::cos(4 * M_PI / 3) * w3;
+      y += std::sin(2 * M_PI / 3) * w2 + std::sin(4 * M_PI / 3) * w3;
+      const double b1 = (s3 * y + 1) / 3, b2 = (-3 * x - s3 * y + 2) / 6, b3 = (3 * x - s3 * y + 2) / 6;
+      out.push_back(0.5 * (1 + (-b2 + b3 - b1)));
+      out.push_back(0.5 * (1 + (-b2 - b3 + b1)));
+    }
+  return out;
+}
+
+// Coefficients of the degree-n Lagrange functions in the PKD basis (inverse
+// Vandermonde), cached per degree.
+static const std::vector<double>& tri_vinv(int n) {
+  static std::mutex mu;
+  static std::map<int, std::vector<double>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(n);
+  if (it != cache.end()) return it->second;
+  const int c = (n + 1) * (n + 2) / 2;
+  std::vector<double> X = tri_lattice(n), A((size_t)c * c), Xi((size_t)c * c, 0.0);
+  for (int p = 0; p < c; p++) {
+    int m = 0;
+    for (int i = 0; i <= n; i++)
+      for (int j = 0; j <= n - i; j++, m++) {
+        double v, dr, ds;
+        pkd(i, j, 2 * X[2 * p] - 1, 2 * X[2 * p + 1] - 1, v, dr, ds);
+        A[(size_t)p * c + m] = v;
+      }
+  }
+  for (int i = 0; i < c; i++) Xi[(size_t)i * c + i] = 1.0;
+  for (int col = 0; col < c; col++) {  // Gauss-Jordan with partial pivoting
+    int piv = col;
+    for (int r = col + 1; r < c; r++)
+      if (std::fabs(A[(size_t)r * c + col]) > std::fabs(A[(size_t)piv * c + col])) piv = r;
+    for (int k = 0; k < c; k++) {
+      std::swap(A[(size_t)col * c + k], A[(size_t)piv * c + k]);
+      std::swap(Xi[(size_t)col * c + k], Xi[(size_t)piv * c + k]);
+    }
+    const double inv = 1.0 / A[(size_t)col * c + col];
+    for (int k = 0; k < c; k++) { A[(size_t)col * c + k] *= inv; Xi[(size_t)col * c + k] *= inv; }
+    for (int r = 0; r < c; r++) {
+      if (r == col) continue;
+      const double f = A[(size_t)r * c + col];
+      if (f == 0.0) continue;
+      for (int k = 0; k < c; k++) {
+        A[(size_t)r * c + k] -= f * A[(size_t)col * c + k];
+        Xi[(size_t)r * c + k] -= f * Xi[(size_t)col * c + k];
+      }
+    }
+  }
+  return cache.emplace(n, std::move(Xi)).first->second;
+}
+
+// HGRAD_TRI_Cn: out[dof*3 + 0] = value, + 1 + k = d/dxi_k.  Returns card.
+static int tab_hgrad_tri(int n, const double* xi, double* out) {
+  const int c = (n + 1) * (n + 2) / 2;
+  if (n == 0) { out[0] = 1.0; out[1] = 0.0; out[2] = 0.0; return 1; }
+  const std::vector<double>& Vi = tri_vinv(n);
+  std::vector<double> pv(c), pr(c), ps(c);
+  int m = 0;
+  for (int i = 0; i <= n; i++)
+    for (int j = 0; j <= n - i; j++, m++) pkd(i, j, 2 * xi[0] - 1, 2 * xi[1] - 1, pv[m], pr[m], ps[m]);
+  for (int k = 0; k < c; k++) {
+    double v = 0, gx = 0, gy = 0;
+    for (int mm = 0; mm < c; mm++) {
+      const double w = Vi[(size_t)mm * c + k];
+      v += pv[mm] * w;
+      gx += pr[mm] * w;
+      gy += ps[mm] * w;
+    }
+    out[k * 3] = v;
+    out[k * 3 + 1] = 2 * gx;
+    out[k * 3 + 2] = 2 * gy;
+  }
+  return c;
+}
+
+// HDIV_TRI_In (RT_n): out[dof*3 + c] = value comp c, + 2 = div.  Returns card n (n + 2).
+static int tab_hdiv_tri(int n, const double* xi, double* out) {
+  const int np = n * (n + 1) / 2;
+  std::vector<double> pv(np), pr(np), ps(np);
+  int m = 0;
+  for (int i = 0; i <= n - 1; i++)
+    for (int j = 0; j <= n - 1 - i; j++, m++) pkd(i, j, 2 * xi[0] - 1, 2 * xi[1] - 1, pv[m], pr[m], ps[m]);
+  int dof = 0;
+  for (int c = 0; c < 2; c++)
+    for (int k = 0; k < np; k++, dof++) {
+      out[dof * 3] = c == 0 ? pv[k] : 0.0;
+      out[dof * 3 + 1] = c == 1 ? pv[k] : 0.0;
+      out[dof * 3 + 2] = 2 * (c == 0 ? pr[k] : ps[k]);
+    }
+  for (int j = 0; j < n; j++, dof++) {
+    const double h = std::pow(xi[0], n - 1 - j) * std::pow(xi[1], j);
+    out[dof * 3] = xi[0] * h;
+    out[dof * 3 + 1] = xi[1] * h;
+    out[dof * 3 + 2] = (n + 1) * h;
+  }
+  return dof;
+}
+
+// Reference-cell bases by topology (tensor cells on [-1,1]^dim, or the triangle).
+static int tab_hgrad_t(int topo, int dim, int p, const double* xi, double* out) {
+  return topo == DPG_TOPO_TRI ? tab_hgrad_tri(p, xi, out) : tab_hgrad(dim, p, xi, out);
+}
+static int tab_hdiv_t(int topo, int dim, int n, const double* xi, double* out) {
+  return topo == DPG_TOPO_TRI ? tab_hdiv_tri(n, xi, out) : tab_hdiv(dim, n, xi, out);
+}
+static int card_hgrad_t(int topo, int dim, int p) {
+  return topo == DPG_TOPO_TRI ? (p + 1) * (p + 2) / 2 : card_hgrad(dim, p);
+}
+static int card_hdiv_t(int topo, int dim, int n) { return topo == DPG_TOPO_TRI ? n * (n + 2) : card_hdiv(dim, n); }
+
+// ----------------------------------------------------------------------------
 // Topology data (shards)
 // ----------------------------------------------------------------------------
 
 struct TopoData {
-  int d, nv, ns;
+  int key, d, nv, ns;
   double v[8][3];
   int sv[6][4];
 };
 
 static bool topo_data(int key, TopoData& t) {
   std::memset(&t, 0, sizeof(t));
+  t.key = key;
   if (key == DPG_TOPO_QUAD) {
     t.d = 2; t.nv = 4; t.ns = 4;
     const double v[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
     for (int a = 0; a < 4; a++) { t.v[a][0] = v[a][0]; t.v[a][1] = v[a][1]; }
     for (int s = 0; s < 4; s++) { t.sv[s][0] = s; t.sv[s][1] = (s + 1) & 3; }
+    return true;
+  }
+  if (key == DPG_TOPO_TRI) {
+    t.d = 2; t.nv = 3; t.ns = 3;
+    const double v[3][2] = {{0, 0}, {1, 0}, {0, 1}};
+    for (int a = 0; a < 3; a++) { t.v[a][0] = v[a][0]; t.v[a][1] = v[a][1]; }
+    for (int s = 0; s < 3; s++) { t.sv[s][0] = s; t.sv[s][1] = (s + 1) % 3; }
+    t.key = key;
     return true;
   }
   if (key == DPG_TOPO_HEX) {
@@ -231,6 +432,10 @@ static bool topo_data(int key, TopoData& t) {
 
 // d(vertex shape)/d(xi) of the (bi/tri)linear geometric map
 static void geom_dshape(const TopoData& t, const double* xi, double* dN) {
+  if (t.key == DPG_TOPO_TRI) {  // affine: N = (1 - xi - eta, xi, eta)
+    dN[0] = -1; dN[1] = -1; dN[2] = 1; dN[3] = 0; dN[4] = 0; dN[5] = 1;
+    return;
+  }
   for (int a = 0; a < t.nv; a++)
     for (int k = 0; k < t.d; k++) {
       double g = 0.5 * t.v[a][k];
@@ -315,18 +520,40 @@ static Rule tensor_rule(int dim, int degree) {
   return r;
 }
 
+// Triangle rule exact to `degree` (any exact rule integrates the polynomial
+// integrands of an affine triangle identically): collapsed Gauss-Legendre,
+// xi = u (1 - v), eta = v on [0,1]^2, weight w_u w_v (1 - v) / 4, u fastest.
+static Rule tri_rule(int degree) {
+  const int nu = degree / 2 + 1, nv = (degree + 1) / 2 + 1;
+  std::vector<double> xu, wu, xv, wv;
+  gauss_rule(nu, xu, wu);
+  gauss_rule(nv, xv, wv);
+  Rule r;
+  r.n = nu * nv;
+  for (int j = 0; j < nv; j++)
+    for (int i = 0; i < nu; i++) {
+      const double u = 0.5 * (1 + xu[i]), v = 0.5 * (1 + xv[j]);
+      r.x.push_back(u * (1 - v));
+      r.x.push_back(v);
+      r.w.push_back(0.25 * wu[i] * wv[j] * (1 - v));
+    }
+  return r;
+}
+
 static int build(HostPlan* P, const dpg_bucket_desc* D) {
   DpgPlanDev& g = P->dev;
   std::memset(&g, 0, sizeof(g));
   TopoData T;
-  if (D->topology == DPG_TOPO_TRI) return fail(DPG_ERR_UNSUPPORTED, "triangle buckets are not supported by this build");
   if (!topo_data(D->topology, T)) return fail(DPG_ERR_INVALID_ARGUMENT, "unknown topology");
+  const int topo = D->topology;
   if (D->n_test < 1 || D->n_test > DPG_MAXV || D->n_trial < 1 || D->n_trial > DPG_MAXV)
-    return fail(DPG_ERR_UNSUPPORTED, "number of test/trial vars out of range (1..8)");
+    return fail(DPG_ERR_UNSUPPORTED, "number of test/trial vars out of range (1..16)");
   const int d = T.d;
   g.d = d; g.nv = T.nv; g.ns = T.ns;
   g.nslots = D->n_slots;
-  Rule rG = tensor_rule(d, D->cub_degree_G), rB = tensor_rule(d, D->cub_degree_B),
+  const bool tri = topo == DPG_TOPO_TRI;
+  Rule rG = tri ? tri_rule(D->cub_degree_G) : tensor_rule(d, D->cub_degree_G),
+       rB = tri ? tri_rule(D->cub_degree_B) : tensor_rule(d, D->cub_degree_B),
        rS = tensor_rule(d - 1, D->cub_degree_side);
   g.QG = rG.n; g.QB = rB.n; g.QS = rS.n;
   if (g.QG > DPG_MAX_QG) return fail(DPG_ERR_UNSUPPORTED, "Gram cubature rule too large");
@@ -397,10 +624,10 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     tv.space = V.space;
     int n = V.poly_order;
     test_n[a] = n;
-    if (V.space == DPG_SPACE_HGRAD) tv.card = card_hgrad(d, n);
+    if (V.space == DPG_SPACE_HGRAD) tv.card = card_hgrad_t(topo, d, n);
     else if (V.space == DPG_SPACE_HDIV) {
       if (n < 1) return fail(DPG_ERR_INVALID_ARGUMENT, "HDIV test order must be >= 1");
-      tv.card = card_hdiv(d, n);
+      tv.card = card_hdiv_t(topo, d, n);
     } else return fail(DPG_ERR_INVALID_ARGUMENT, "test vars must be HGRAD or HDIV");
     // rows padded to pairs of 8-row tiles (16x8 mma blocks never straddle two vars)
     const int rows = (tv.card + 15) & ~15;
@@ -428,8 +655,8 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       for (int a = 0; a < g.ntest; a++) {
         const DpgTestVar& tv = g.test[a];
         std::vector<double> tmp((size_t)tv.card * (d + 1));
-        if (tv.space == DPG_SPACE_HGRAD) tab_hgrad(d, test_n[a], pts + (size_t)q * d, tmp.data());
-        else tab_hdiv(d, test_n[a], pts + (size_t)q * d, tmp.data());
+        if (tv.space == DPG_SPACE_HGRAD) tab_hgrad_t(topo, d, test_n[a], pts + (size_t)q * d, tmp.data());
+        else tab_hdiv_t(topo, d, test_n[a], pts + (size_t)q * d, tmp.data());
         double* dst = &out[(size_t)q * g.featstride + tv.foff];
         for (int i = 0; i < tv.card; i++)
           for (int m = 0; m <= d; m++) dst[(size_t)m * tv.ldA + i] = tmp[(size_t)i * (d + 1) + m];
@@ -460,7 +687,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       int p = V.poly_order - 1;
       if (p < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "field H1Order must be >= 1");
       tr.ncomp = (V.space == DPG_SPACE_VECTOR_HVOL) ? d : 1;
-      tr.card_comp = card_hgrad(d, p);
+      tr.card_comp = card_hgrad_t(topo, d, p);
       tr.user_off = user_col;
       tr.dev_off = fcount;
       fcount += tr.ncomp * tr.card_comp;
@@ -468,11 +695,11 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       std::vector<double> tb((size_t)g.QBpad * tr.card_comp), ts((size_t)g.ns * g.QSpad * tr.card_comp);
       std::vector<double> tmp((size_t)tr.card_comp * (1 + d));
       for (int q = 0; q < g.QBpad; q++) {
-        tab_hgrad(d, p, &xB[(size_t)q * d], tmp.data());
+        tab_hgrad_t(topo, d, p, &xB[(size_t)q * d], tmp.data());
         for (int i = 0; i < tr.card_comp; i++) tb[(size_t)q * tr.card_comp + i] = tmp[(size_t)i * (1 + d)];
       }
       for (int q = 0; q < g.ns * g.QSpad; q++) {
-        tab_hgrad(d, p, &sidepts[(size_t)q * d], tmp.data());
+        tab_hgrad_t(topo, d, p, &sidepts[(size_t)q * d], tmp.data());
         for (int i = 0; i < tr.card_comp; i++) ts[(size_t)q * tr.card_comp + i] = tmp[(size_t)i * (1 + d)];
       }
       tr.tabB = upload(P, tb);
@@ -571,22 +798,30 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     while (e < g.nipent && g.ipent[e].row < r) e++;
     g.rowstart[r] = e;
   }
-  // var pairs (a >= b), h block offsets
+  // var pairs (a >= b) that some IP row couples (the others' G blocks are zero), h block offsets
   {
+    std::vector<int> coupled(g.ntest * g.ntest, 0);
+    for (int r = 0; r < g.niprows; r++)
+      for (int e = g.rowstart[r]; e < g.rowstart[r + 1]; e++)
+        for (int e2 = g.rowstart[r]; e2 < g.rowstart[r + 1]; e2++)
+          coupled[(g.ipent[e].gslot >> 2) * g.ntest + (g.ipent[e2].gslot >> 2)] = 1;
+    std::vector<int> pidx(g.ntest * g.ntest, -1);
     int off = 0, np = 0;
     for (int a = 0; a < g.ntest; a++)
       for (int b = 0; b <= a; b++) {
+        if (!coupled[a * g.ntest + b]) continue;
         if (np >= DPG_MAX_PAIRS) return fail(DPG_ERR_UNSUPPORTED, "too many test var pairs");
         g.pair_a[np] = a;
         g.pair_b[np] = b;
         g.hoff[np] = off;
+        pidx[a * g.ntest + b] = np;
         off += 4 * g.test[b].ldA;
         np++;
       }
     g.npairs = np;
     g.hstride = off;
-    auto pair_index = [&](int a, int b) { return a * (a + 1) / 2 + b; };
     std::vector<DpgGTile> tiles;
+    std::vector<char> covered(g.NBT * (g.NBT + 1) / 2, 0);
     for (int a = 0; a < g.ntest; a++)
       for (int rp = 0; rp < g.test[a].ntiles; rp += 2) {
         const int I = g.test[a].ntile0 + rp;
@@ -594,17 +829,25 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
           for (int jj = 0; jj < g.test[b].ntiles; jj++) {
             const int J = g.test[b].ntile0 + jj;
             if (J > I + 1) continue;
+            if (pidx[a * g.ntest + b] < 0) continue;
+            if (J <= I) covered[I * (I + 1) / 2 + J] = 1;
+            covered[(I + 1) * (I + 2) / 2 + J] = 1;
             DpgGTile t;
             t.I = (int16_t)I; t.J = (int16_t)J;
             t.aoff = g.test[a].foff + rp * 8;
             t.lda = (int16_t)g.test[a].ldA;
-            t.boff = g.hoff[pair_index(a, b)] + jj * 8;
+            t.boff = g.hoff[pidx[a * g.ntest + b]] + jj * 8;
             t.ldb = (int16_t)g.test[b].ldA;
             tiles.push_back(t);
           }
       }
     g.ngb = (int)tiles.size();
     g.ngt = g.NBT * (g.NBT + 1) / 2;
+    std::vector<int> gz;  // lower tiles no block writes (uncoupled var pairs)
+    for (int u = 0; u < g.ngt; u++)
+      if (!covered[u]) gz.push_back(u);
+    g.ngz = (int)gz.size();
+    g.gzero = upload_i(P, gz);
     if ((g.ngb + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_GT) return fail(DPG_ERR_UNSUPPORTED, "too many G blocks");
     void* p = nullptr;
     if (cudaMalloc(&p, tiles.size() * sizeof(DpgGTile)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
@@ -939,15 +1182,15 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     }
 
   // ---- shared memory layout (doubles) ----------------------------------------
-  {
+  for (g.chg = DPG_CHG;; g.chg /= 2) {
     auto al = [](int x) { return (x + 15) & ~15; };  // 128-byte aligned regions
     int o = 0;
     // Gram phase
-    g.g_fref0 = o; o += al(DPG_CHG * g.featstride);
-    g.g_fref1 = o; o += al(DPG_CHG * g.featstride);
+    g.g_fref0 = o; o += al(g.chg * g.featstride);
+    g.g_fref1 = o; o += al(g.chg * g.featstride);
     g.g_h = o;
     g.g_beta = o;  // per-point IP rows in reference slots; dead before the first h chunk
-    o += al(std::max(DPG_CHG * g.hstride, g.QGpad * g.niprows * 4 * g.ntest));
+    o += al(std::max(g.chg * g.hstride, g.QGpad * g.niprows * 4 * g.ntest));
     g.g_geo = o; o += al(g.QGpad * 24);
     g.g_D = o; o += al(g.QGpad * g.npairs * 16);
     int gphase = o;
@@ -994,9 +1237,12 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     g.sm_nodes = g.sm_tiles + al((g.ngb * (int)sizeof(DpgGTile) + 7) / 8);
     g.sm_invd = g.sm_nodes + 192;
     g.sm_total = g.sm_invd + al(std::max(g.Np, g.Mp));
-    if ((size_t)g.sm_total * 8 > 232448)
+    if ((size_t)g.sm_total * 8 > 232448) {
+      if (g.chg > DPG_CHG / 2) continue;  // retry with half-size Gram chunks
       return fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
+    }
     g.scratch_per_cta = (size_t)g.MBT * g.NBT * 64;
+    break;
   }
   // info
   dpg_plan_info& I = P->info;

@@ -606,8 +606,8 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
   double* Dm = sm + P.g_D;  // [q][pair][16]
   double* hb = sm + P.g_h;
   double* GT = sm + P.sm_gt;
-  const int nch = P.QGpad / DPG_CHG;
-  const uint32_t chunk_bytes = (uint32_t)(DPG_CHG * P.featstride * sizeof(double));
+  const int nch = P.QGpad / P.chg;
+  const uint32_t chunk_bytes = (uint32_t)(P.chg * P.featstride * sizeof(double));
   if (tid == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&mbar_s[0], chunk_bytes);
@@ -678,7 +678,7 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
       if (c + 1 < nch) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(&mbar_s[buf ^ 1], chunk_bytes);
-        bulk_g2s(sm + (buf ? P.g_fref0 : P.g_fref1), P.frefG + (size_t)(c + 1) * DPG_CHG * P.featstride,
+        bulk_g2s(sm + (buf ? P.g_fref0 : P.g_fref1), P.frefG + (size_t)(c + 1) * P.chg * P.featstride,
                  chunk_bytes, &mbar_s[buf ^ 1]);
       }
       if (!mbar_wait(&mbar_s[buf], X.phase[buf] & 1)) flag_s[2] = 1;
@@ -691,11 +691,11 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
       while (r >= P.test[P.pair_b[p]].ntiles) { r -= P.test[P.pair_b[p]].ntiles; p++; }
       const int b = P.pair_b[p];
       const int ld = P.test[b].ldA;
-      const double* dp = Dm + ((size_t)c * DPG_CHG * P.npairs + p) * 16 + g * 4 + t;
+      const double* dp = Dm + ((size_t)c * P.chg * P.npairs + p) * 16 + g * 4 + t;
       const double* fp = fref + P.test[b].foff + t * ld + r * 8 + g;
       double* hp = hb + P.hoff[p] + g * ld + r * 8 + 2 * t;
-#pragma unroll
-      for (int lq = 0; lq < DPG_CHG; lq++) {
+#pragma unroll 4
+      for (int lq = 0; lq < P.chg; lq++) {
         const double av = (g < 4) ? dp[lq * P.npairs * 16] : 0.0;
         const double bv = fp[lq * P.featstride];
         double2 hc = make_double2(0.0, 0.0);
@@ -706,7 +706,7 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
     __syncthreads();
     // m16n8k16 over the owned blocks: one k16 step = 4 points x 4 slots
 #pragma unroll 1
-    for (int s4 = 0; s4 < DPG_CHG; s4 += 4) {
+    for (int s4 = 0; s4 < P.chg; s4 += 4) {
       const double* fa = fref + s4 * P.featstride;
       const double* hq = hb + s4 * P.hstride;
       uint32_t prevA = 0xffffffffu;
@@ -732,7 +732,9 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
     }
     __syncthreads();
   }
-  // accumulators -> tile-lower shared storage (overlaps the staging area)
+  // accumulators -> tile-lower shared storage (overlaps the staging area); tiles of
+  // uncoupled var pairs are zero
+  for (int e = tid; e < P.ngz * 64; e += NT) GT[P.gzero[e >> 6] * 64 + (e & 63)] = 0.0;
 #pragma unroll
   for (int u = 0; u < GTM; u++) {
     if (u < ntw) {

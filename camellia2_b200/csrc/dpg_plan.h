@@ -20,7 +20,7 @@
 #pragma once
 #include <stdint.h>
 
-#define DPG_MAXV 8        // max test vars / trial vars per bucket
+#define DPG_MAXV 16       // max test vars / trial vars per bucket
 #define DPG_MAX_BF 96     // max scalar bilinear products (after side expansion)
 #define DPG_MAX_IP 64     // max inner-product entries
 #define DPG_MAX_RHS 8
@@ -30,7 +30,7 @@
 #define DPG_MAX_PAIRS 36  // test var pairs a >= b
 #define DPG_NWARPS 16
 #define DPG_NTHREADS (DPG_NWARPS * 32)
-#define DPG_CHG 8         // Gram quadrature points per staged chunk
+#define DPG_CHG 8         // Gram quadrature points per staged chunk (4 when shared memory is short)
 #define DPG_MAX_CHB 16    // max B quadrature points per staged chunk
 #define DPG_MAX_BT 12     // max terms feeding one B block
 #define DPG_MAX_BTW 12    // max active B tiles per warp per segment
@@ -146,6 +146,9 @@ struct DpgPlanDev {
   int ngt;                  // lower 8x8 tiles of G: NBT (NBT + 1) / 2
   int ngb;                  // 16x8 G blocks
   const DpgGTile* gtiles;   // [ngb]
+  int ngz;                  // lower tiles of G that no block writes (uncoupled test var pairs)
+  const int* gzero;         // [ngz] their indices I (I + 1) / 2 + J
+  int chg;                  // Gram points per staged chunk (DPG_CHG or DPG_CHG / 2)
   int featstride;           // doubles per point of staged slots (sum over vars of 4*ldA)
   int hstride;              // doubles per point of staged h blocks (sum over pairs)
   const double* frefG;      // [QGpad][featstride]

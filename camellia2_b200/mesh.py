@@ -36,6 +36,45 @@ def quad_grid(nx, ny, jitter=0.0, seed=1, extent=(1.0, 1.0)):
     return np.ascontiguousarray(nodes), par
 
 
+def tri_grid(nx, ny, jitter=0.0, seed=1, extent=(1.0, 1.0)):
+    """nx*ny quads on [0,Lx]x[0,Ly], each cut along its diagonal into two
+    counter-clockwise triangles (v00, v10, v11) and (v00, v11, v01); interior nodes
+    jittered by U[-jitter*h, jitter*h].  Side s of a triangle joins its vertices s
+    and s+1 (shards Triangle<3>).  Side parity: +1 on the boundary and for the
+    lower cell id of a neighbour pair, -1 for the higher.  Returns nodes (C,3,2),
+    parity (C,3)."""
+    rng = np.random.default_rng(seed)
+    hx, hy = extent[0] / nx, extent[1] / ny
+    X, Y = np.meshgrid(np.arange(nx + 1) * hx, np.arange(ny + 1) * hy, indexing="ij")
+    if jitter:
+        jx = rng.uniform(-jitter * hx, jitter * hx, size=X.shape)
+        jy = rng.uniform(-jitter * hy, jitter * hy, size=Y.shape)
+        interior = np.zeros_like(X, dtype=bool)
+        interior[1:-1, 1:-1] = True
+        X = X + np.where(interior, jx, 0.0)
+        Y = Y + np.where(interior, jy, 0.0)
+    vid = lambda i, j: i * (ny + 1) + j  # noqa: E731
+    cells = []
+    for j in range(ny):
+        for i in range(nx):
+            v00, v10, v11, v01 = vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)
+            cells.append((v00, v10, v11))
+            cells.append((v00, v11, v01))
+    cells = np.array(cells)
+    P = np.stack([X.reshape(-1), Y.reshape(-1)], axis=-1)
+    nodes = P[cells]
+    owner = {}
+    par = np.ones((len(cells), 3), dtype=np.int8)
+    for c, tri in enumerate(cells):
+        for s in range(3):
+            key = tuple(sorted((tri[s], tri[(s + 1) % 3])))
+            if key in owner:
+                par[c, s] = -1  # the other cell has the lower id
+            else:
+                owner[key] = c
+    return np.ascontiguousarray(nodes), par
+
+
 def hex_grid(nx, ny, nz, jitter=0.0, seed=1, extent=(1.0, 1.0, 1.0)):
     """nx*ny*nz hexes; interior nodes jittered by U[-jitter*h, jitter*h].
     Returns nodes (C,8,3) float64 and parity (C,6) int8."""

@@ -210,11 +210,193 @@ static void geom_shape(const Topo& t, const double* xi, double* N, double* dN /*
 // Bases: tabulation of reference values at points
 // ----------------------------------------------------------------------------
 
+// ----------------------------------------------------------------------------
+// Triangle bases.  Intrepid's Basis_HGRAD_TRI_Cn_FEM (POINTTYPE_WARPBLEND,
+// BasisFactory.cpp:198-350) is a Lagrange basis on the warp & blend lattice; the
+// lattice is restated from the published construction (Warburton 2006;
+// Hesthaven & Warburton, "Nodal Discontinuous Galerkin Methods", Nodes2D with the
+// optimized alpha table), and the Lagrange functions are built through the
+// orthonormal Proriol-Koornwinder-Dubiner (PKD) basis on the biunit triangle.
+// Basis_HDIV_TRI_In_FEM spans Raviart-Thomas RT_n (card n(n+2)); this file uses a
+// modal basis of the same space: (p, 0), (0, p) for p in P_{n-1}, then x h for
+// the homogeneous monomials h of degree n-1.  A test-space basis change leaves
+// K, l and S unchanged (K = B^T G^-1 B is invariant under B -> T^T B, G -> T^T G T).
+// ----------------------------------------------------------------------------
+
+// Orthonormal Jacobi polynomial P_n^{(a,b)}(x) on [-1,1] (weight (1-x)^a (1+x)^b).
+static double jacobi(double x, double a, double b, int n) {
+  double g0 = std::pow(2.0, a + b + 1) / (a + b + 1) * std::tgamma(a + 1) * std::tgamma(b + 1) / std::tgamma(a + b + 1);
+  double p0 = 1.0 / std::sqrt(g0);
+  if (n == 0) return p0;
+  double g1 = (a + 1) * (b + 1) / (a + b + 3) * g0;
+  double p1 = ((a + b + 2) * x / 2 + (a - b) / 2) / std::sqrt(g1);
+  if (n == 1) return p1;
+  double aold = 2.0 / (2 + a + b) * std::sqrt((a + 1) * (b + 1) / (a + b + 3));
+  for (int i = 1; i < n; i++) {
+    double h1 = 2.0 * i + a + b;
+    double anew = 2.0 / (h1 + 2) * std::sqrt((i + 1) * (i + 1 + a + b) * (i + 1 + a) * (i + 1 + b) / (h1 + 1) / (h1 + 3));
+    double bnew = -(a * a - b * b) / h1 / (h1 + 2);
+    double p2 = (-aold * p0 + (x - bnew) * p1) / anew;
+    p0 = p1;
+    p1 = p2;
+    aold = anew;
+  }
+  return p1;
+}
+static double jacobi_d(double x, double a, double b, int n) {
+  return n == 0 ? 0.0 : std::sqrt(n * (n + a + b + 1)) * jacobi(x, a + 1, b + 1, n - 1);
+}
+
+// PKD mode (i, j) and its (r, s) derivatives at a point of the biunit triangle.
+static void pkd_mode(int i, int j, double r, double s, double& v, double& vr, double& vs) {
+  double a = (std::fabs(s - 1.0) > 1e-14) ? 2.0 * (1.0 + r) / (1.0 - s) - 1.0 : -1.0, b = s;
+  double fa = jacobi(a, 0, 0, i), dfa = jacobi_d(a, 0, 0, i);
+  double gb = jacobi(b, 2 * i + 1, 0, j), dgb = jacobi_d(b, 2 * i + 1, 0, j);
+  double hb = 0.5 * (1.0 - b);
+  v = std::sqrt(2.0) * fa * gb * std::pow(1.0 - b, i);
+  double dr = dfa * gb, ds = dfa * gb * 0.5 * (1.0 + a);
+  if (i > 0) { dr *= std::pow(hb, i - 1); ds *= std::pow(hb, i - 1); }
+  double tmp = dgb * std::pow(hb, i);
+  if (i > 0) tmp -= 0.5 * i * gb * std::pow(hb, i - 1);
+  ds += fa * tmp;
+  const double sc = std::pow(2.0, i + 0.5);
+  vr = dr * sc;
+  vs = ds * sc;
+}
+
+// Warp & blend lattice of degree N on the reference triangle (0,0),(1,0),(0,1):
+// Np = (N+1)(N+2)/2 points, bottom row first (eta = 0, xi ascending).
+static vector<double> warp_blend_tri(int N) {
+  static const double alpopt[15] = {0.0000, 0.0000, 1.4152, 0.1001, 0.2751, 0.9800, 1.0999, 1.2832,
+                                    1.3648, 1.4773, 1.4959, 1.5743, 1.5770, 1.6223, 1.6258};
+  const double alpha = N < 16 ? alpopt[N - 1] : 5.0 / 3.0;
+  vector<double> gll(N + 1);
+  gauss_lobatto(N, gll.data());
+  auto warpf = [&](double r) {
+    // interpolant on equispaced nodes of the GLL displacement, divided by 1 - r^2
+    double w = 0.0;
+    for (int i = 0; i <= N; i++) {
+      double xi_eq = -1.0 + 2.0 * i / N, l = 1.0;
+      for (int j = 0; j <= N; j++)
+        if (j != i) l *= (r - (-1.0 + 2.0 * j / N)) / (xi_eq - (-1.0 + 2.0 * j / N));
+      w += (gll[i] - xi_eq) * l;
+    }
+    return std::fabs(r) < 1.0 - 1e-10 ? w / (1.0 - r * r) : 0.0;
+  };
+  vector<double> out;
+  const double c2 = std::cos(2 * M_PI / 3), s2 = std::sin(2 * M_PI / 3);
+  const double c4 = std::cos(4 * M_PI / 3), s4 = std::sin(4 * M_PI / 3);
+  for (int n = 0; n <= N; n++)
+    for (int m = 0; m <= N - n; m++) {
+      double L1 = (double)n / N, L3 = (double)m / N, L2 = 1.0 - L1 - L3;
+      double x = -L2 + L3, y = (-L2 - L3 + 2 * L1) / std::sqrt(3.0);
+      double w1 = 4 * L2 * L3 * warpf(L3 - L2) * (1 + (alpha * L1) * (alpha * L1));
+      double w2 = 4 * L1 * L3 * warpf(L1 - L3) * (1 + (alpha * L2) * (alpha * L2));
+      double w3 = 4 * L1 * L2 * warpf(L2 - L1) * (1 + (alpha * L3) * (alpha * L3));
+      x += w1 + c2 * w2 + c4 * w3;
+      y += s2 * w2 + s4 * w3;
+      // equilateral -> biunit (r, s) -> reference (xi, eta)
+      double b1 = (std::sqrt(3.0) * y + 1) / 3, b2 = (-3 * x - std::sqrt(3.0) * y + 2) / 6,
+             b3 = (3 * x - std::sqrt(3.0) * y + 2) / 6;
+      double r = -b2 + b3 - b1, s = -b2 - b3 + b1;
+      out.push_back(0.5 * (1 + r));
+      out.push_back(0.5 * (1 + s));
+    }
+  return out;
+}
+
+// Inverse of a dense n x n matrix (Gauss-Jordan, partial pivoting).
+static vector<double> invert(vector<double> A, int n) {
+  vector<double> X(n * n, 0.0);
+  for (int i = 0; i < n; i++) X[i * n + i] = 1.0;
+  for (int c = 0; c < n; c++) {
+    int piv = c;
+    for (int r = c + 1; r < n; r++)
+      if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+    for (int k = 0; k < n; k++) { std::swap(A[c * n + k], A[piv * n + k]); std::swap(X[c * n + k], X[piv * n + k]); }
+    double inv = 1.0 / A[c * n + c];
+    for (int k = 0; k < n; k++) { A[c * n + k] *= inv; X[c * n + k] *= inv; }
+    for (int r = 0; r < n; r++) {
+      if (r == c) continue;
+      double f = A[r * n + c];
+      if (f == 0.0) continue;
+      for (int k = 0; k < n; k++) { A[r * n + k] -= f * A[c * n + k]; X[r * n + k] -= f * X[c * n + k]; }
+    }
+  }
+  return X;
+}
+
+// Lagrange basis of degree N on the warp & blend lattice: phi_k = sum_m psi_m Vinv[m][k].
+struct TriLagrange {
+  int N = 0, card = 1;
+  vector<double> vinv;
+  void init(int n) {
+    N = n;
+    card = (n + 1) * (n + 2) / 2;
+    if (n == 0) return;
+    vector<double> X = warp_blend_tri(n), V((size_t)card * card);
+    for (int p = 0; p < card; p++) {
+      int m = 0;
+      for (int i = 0; i <= n; i++)
+        for (int j = 0; j <= n - i; j++, m++) {
+          double v, vr, vs;
+          pkd_mode(i, j, 2 * X[2 * p] - 1, 2 * X[2 * p + 1] - 1, v, vr, vs);
+          V[(size_t)p * card + m] = v;
+        }
+    }
+    vinv = invert(V, card);
+  }
+  // values and reference (xi, eta) gradients of all card functions
+  void eval(const double* xi, double* val, double* grad) const {
+    if (N == 0) {
+      if (val) val[0] = 1.0;
+      if (grad) { grad[0] = 0.0; grad[1] = 0.0; }
+      return;
+    }
+    vector<double> pv(card), pr(card), ps(card);
+    int m = 0;
+    for (int i = 0; i <= N; i++)
+      for (int j = 0; j <= N - i; j++, m++) pkd_mode(i, j, 2 * xi[0] - 1, 2 * xi[1] - 1, pv[m], pr[m], ps[m]);
+    for (int k = 0; k < card; k++) {
+      double v = 0, gx = 0, gy = 0;
+      for (int mm = 0; mm < card; mm++) {
+        double c = vinv[(size_t)mm * card + k];
+        v += pv[mm] * c;
+        gx += pr[mm] * c;
+        gy += ps[mm] * c;
+      }
+      if (val) val[k] = v;
+      if (grad) { grad[2 * k] = 2 * gx; grad[2 * k + 1] = 2 * gy; }  // d/dxi = 2 d/dr
+    }
+  }
+};
+
+// Modal RT_n basis on the reference triangle: values (2 per function) and divergence.
+static void tri_rt_eval(int n, const double* xi, double* val, double* div) {
+  const int np = n * (n + 1) / 2;  // dim P_{n-1}
+  vector<double> pv(np), pr(np), ps(np);
+  int m = 0;
+  for (int i = 0; i <= n - 1; i++)
+    for (int j = 0; j <= n - 1 - i; j++, m++) pkd_mode(i, j, 2 * xi[0] - 1, 2 * xi[1] - 1, pv[m], pr[m], ps[m]);
+  int dof = 0;
+  for (int c = 0; c < 2; c++)
+    for (int k = 0; k < np; k++, dof++) {
+      if (val) { val[2 * dof] = c == 0 ? pv[k] : 0.0; val[2 * dof + 1] = c == 1 ? pv[k] : 0.0; }
+      if (div) div[dof] = 2 * (c == 0 ? pr[k] : ps[k]);
+    }
+  for (int j = 0; j < n; j++, dof++) {
+    double h = std::pow(xi[0], n - 1 - j) * std::pow(xi[1], j);
+    if (val) { val[2 * dof] = xi[0] * h; val[2 * dof + 1] = xi[1] * h; }
+    if (div) div[dof] = (n + 1) * h;
+  }
+}
+
 struct Basis {
   int topo = 0, space = 0, n = 0;  // n: Cn / In order of the Intrepid basis
   int d = 0, card = 0, rank = 0;   // rank 0 scalar, 1 vector (d comps)
   int ncomp = 1;                   // VECTOR_HVOL copies
   Nodal1D closed, open;            // 1D families
+  TriLagrange tri;                 // triangle HGRAD
   // Tabulate at point xi: val[card*vdim], grad[card*d] (HGRAD-type), div[card]
   void eval(const double* xi, double* val, double* grad, double* div) const;
 };
@@ -228,6 +410,8 @@ struct TriPoly {
 };
 
 static int tensor_card(const Basis& b) {
+  if (b.topo == DPG_TOPO_TRI)
+    return b.space == DPG_SPACE_HDIV ? b.n * (b.n + 2) : (b.n + 1) * (b.n + 2) / 2 * b.ncomp;
   if (b.topo == DPG_TOPO_QUAD || b.topo == DPG_TOPO_HEX || b.topo == 0) {
     int m = b.closed.size();
     if (b.space == DPG_SPACE_HDIV) {
@@ -245,6 +429,12 @@ static Basis make_basis(int topo, int space, int n, int ncomp = 1) {
   Basis b;
   b.topo = topo; b.space = space; b.n = n; b.ncomp = ncomp;
   b.d = (topo == DPG_TOPO_HEX) ? 3 : (topo == 0 ? 1 : 2);  // topo 0 = line
+  if (topo == DPG_TOPO_TRI) {
+    b.rank = space == DPG_SPACE_HDIV ? 1 : 0;
+    if (space != DPG_SPACE_HDIV) b.tri.init(n);
+    b.card = tensor_card(b);
+    return b;
+  }
   if (space == DPG_SPACE_HDIV) {
     b.rank = 1;
     b.closed.closed(n);
@@ -259,6 +449,22 @@ static Basis make_basis(int topo, int space, int n, int ncomp = 1) {
 
 void Basis::eval(const double* xi, double* val, double* grad, double* div) const {
   int d_ = d;
+  if (topo == DPG_TOPO_TRI) {
+    if (space == DPG_SPACE_HDIV) {
+      tri_rt_eval(n, xi, val, div);
+      return;
+    }
+    const int nper = tri.card;
+    vector<double> v(nper), gr(2 * nper);
+    tri.eval(xi, v.data(), gr.data());
+    for (int c = 0; c < ncomp; c++)
+      for (int k = 0; k < nper; k++) {
+        const int dof = c * nper + k;
+        if (val) val[dof] = v[k];
+        if (grad) { grad[dof * 2] = gr[2 * k]; grad[dof * 2 + 1] = gr[2 * k + 1]; }
+      }
+    return;
+  }
   if (space != DPG_SPACE_HDIV) {
     int m = closed.size();
     int nper = 1;
@@ -352,6 +558,27 @@ static Rule tensor_gauss(int dim, int degree) {
   return r;
 }
 
+// Triangle rule exact to `degree` (Intrepid uses a symmetric rule of the same
+// degree; on affine triangles every integrand is a polynomial of at most that
+// degree, so any exact rule gives the same integrals): collapsed Gauss-Legendre,
+// xi = u (1 - v), eta = v, weight w_u w_v (1 - v) / 4 on [0,1]^2, u fastest.
+static Rule tri_rule(int degree) {
+  const int nu = degree / 2 + 1, nv = (degree + 1) / 2 + 1;
+  vector<double> xu(nu), wu(nu), xv(nv), wv(nv);
+  gauss_legendre(nu, xu.data(), wu.data());
+  gauss_legendre(nv, xv.data(), wv.data());
+  Rule r;
+  r.dim = 2;
+  for (int j = 0; j < nv; j++)
+    for (int i = 0; i < nu; i++) {
+      double u = 0.5 * (1 + xu[i]), v = 0.5 * (1 + xv[j]);
+      r.pts.push_back(u * (1 - v));
+      r.pts.push_back(v);
+      r.wts.push_back(0.25 * wu[i] * wv[j] * (1 - v));
+    }
+  return r;
+}
+
 // ----------------------------------------------------------------------------
 // Plan
 // ----------------------------------------------------------------------------
@@ -414,7 +641,6 @@ static bool build_plan(Plan& P, const dpg_bucket_desc* desc) {
   if (desc->n_rhs) P.rhs.assign(desc->rhs, desc->rhs + desc->n_rhs);
   P.topo = make_topo(desc->topology);
   if (P.topo.d == 0) { g_err = "unknown topology"; return false; }
-  if (desc->topology == DPG_TOPO_TRI) { g_err = "oracle: triangle bases not implemented"; return false; }
   P.d = P.topo.d;
   int side_topo = (P.d == 2) ? 0 : DPG_TOPO_QUAD;
   // test vars
@@ -455,8 +681,9 @@ static bool build_plan(Plan& P, const dpg_bucket_desc* desc) {
   P.nf = 0;
   for (int x : P.is_field) P.nf += x;
   P.nt = P.M - P.nf;
-  P.rG = tensor_gauss(P.d, desc->cub_degree_G);
-  P.rB = tensor_gauss(P.d, desc->cub_degree_B);
+  const bool tri = desc->topology == DPG_TOPO_TRI;
+  P.rG = tri ? tri_rule(desc->cub_degree_G) : tensor_gauss(P.d, desc->cub_degree_G);
+  P.rB = tri ? tri_rule(desc->cub_degree_B) : tensor_gauss(P.d, desc->cub_degree_B);
   P.rS = tensor_gauss(P.d - 1, desc->cub_degree_side);
   // map side points to the volume reference cell
   P.side_pts.resize(P.topo.nsides);
@@ -1047,6 +1274,21 @@ int orc_cubature(int dim, int degree, double* pts, double* wts) {
   if (pts) std::copy(r.pts.begin(), r.pts.end(), pts);
   if (wts) std::copy(r.wts.begin(), r.wts.end(), wts);
   return r.npts();
+}
+
+// Triangle rule exact to `degree` on the reference triangle.
+int orc_tri_cubature(int degree, double* pts, double* wts) {
+  Rule r = tri_rule(degree);
+  if (pts) std::copy(r.pts.begin(), r.pts.end(), pts);
+  if (wts) std::copy(r.wts.begin(), r.wts.end(), wts);
+  return r.npts();
+}
+
+// Warp & blend lattice of degree n (the nodes of the triangle HGRAD basis).
+int orc_tri_nodes(int n, double* pts) {
+  vector<double> x = warp_blend_tri(n);
+  if (pts) std::copy(x.begin(), x.end(), pts);
+  return (int)x.size() / 2;
 }
 
 }  // extern "C"

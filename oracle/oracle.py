@@ -38,6 +38,8 @@ def lib():
         L.orc_trial_is_field.argtypes = [ct.c_void_p, ct.c_void_p]
         L.orc_basis_tabulate.argtypes = [ct.c_int] * 4 + [ct.c_void_p] * 4
         L.orc_cubature.argtypes = [ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p]
+        L.orc_tri_cubature.argtypes = [ct.c_int, ct.c_void_p, ct.c_void_p]
+        L.orc_tri_nodes.argtypes = [ct.c_int, ct.c_void_p]
         L.orc_last_error.restype = ct.c_char_p
         _LIB = L
     return _LIB
@@ -144,3 +146,17 @@ def cubature(dim, degree):
     pts, wts = np.zeros((n, dim)), np.zeros(n)
     lib().orc_cubature(dim, degree, _p(pts), _p(wts))
     return pts, wts
+
+
+def tri_cubature(degree):
+    n = lib().orc_tri_cubature(degree, None, None)
+    pts, wts = np.zeros((n, 2)), np.zeros(n)
+    lib().orc_tri_cubature(degree, _p(pts), _p(wts))
+    return pts, wts
+
+
+def tri_nodes(n):
+    m = lib().orc_tri_nodes(n, None)
+    pts = np.zeros((m, 2))
+    lib().orc_tri_nodes(n, _p(pts))
+    return pts

@@ -25,6 +25,27 @@ def cdr2d(k, dk, nx=3, ny=3, jitter=0.0, seed=1):
     return form, bucket, nodes, par
 
 
+def stokes2d(k, dk, nx=2, ny=2, jitter=0.1, seed=1):
+    form = fm.StokesVGPFormulation(2)
+    bucket = form.bucket(abi.TOPO_QUAD, k, dk)
+    nodes, par = mesh.quad_grid(nx, ny, jitter, seed=seed)
+    return form, bucket, nodes, par
+
+
+def poisson_tri(k, dk, nx=2, ny=2, jitter=0.15, seed=1):
+    form = fm.PoissonFormulation(2)
+    bucket = form.bucket(abi.TOPO_TRI, k, dk)
+    nodes, par = mesh.tri_grid(nx, ny, jitter, seed=seed)
+    return form, bucket, nodes, par
+
+
+def stokes_tri(k, dk, nx=2, ny=1, jitter=0.1, seed=1):
+    form = fm.StokesVGPFormulation(2)
+    bucket = form.bucket(abi.TOPO_TRI, k, dk)
+    nodes, par = mesh.tri_grid(nx, ny, jitter, seed=seed)
+    return form, bucket, nodes, par
+
+
 def coeffs_for(bucket, info, C, seed=2):
     if bucket.n_slots == 0:
         return None

@@ -6,7 +6,7 @@ import pytest
 
 from camellia2_b200 import abi, formulation as fm, mesh
 from tests.conftest import rel_fro
-from tests.helpers import cdr2d, coeffs_for, poisson2d, poisson3d
+from tests.helpers import poisson_tri, stokes_tri, cdr2d, coeffs_for, poisson2d, poisson3d
 
 
 def test_poisson_graph_norm_terms():
@@ -219,3 +219,76 @@ def test_optimal_test_algebra(oracle_mod, builder, args):
         s = l[~f] - Bc.T @ np.linalg.solve(D, l[f])
         assert rel_fro(out["S"][c], S) < 1e-10
         assert rel_fro(out["s"][c], s) < 1e-10
+
+
+def _tri_trial_interpolant(oracle_mod, nodes_c, par_c, u, grad_u, k):
+    """Trial coefficients of an exact solution on one triangle (Poisson UW): fields at
+    the warp & blend lattice of degree k-1, traces at Gauss-Lobatto points of each edge
+    (edge s runs from vertex s to vertex s+1), sigma_n_hat = parity * sigma.n."""
+    from numpy.polynomial.legendre import Legendre
+
+    def gll(p):
+        if p == 0:
+            return np.array([0.0])
+        if p == 1:
+            return np.array([-1.0, 1.0])
+        return np.concatenate([[-1.0], np.sort(Legendre.basis(p).deriv().roots().real), [1.0]])
+
+    V = nodes_c
+    xmap = lambda xi: V[0] + xi[..., :1] * (V[1] - V[0]) + xi[..., 1:2] * (V[2] - V[0])  # noqa: E731
+    X = xmap(oracle_mod.tri_nodes(k - 1))
+    coeffs = list(u(X))
+    G = grad_u(X)
+    coeffs += list(G[:, 0]) + list(G[:, 1])
+    for s in range(3):
+        a, b = V[s], V[(s + 1) % 3]
+        for t in gll(k):
+            coeffs.append(u((0.5 * (1 - t) * a + 0.5 * (1 + t) * b)[None, :])[0])
+    for s in range(3):
+        a, b = V[s], V[(s + 1) % 3]
+        T = b - a
+        n = np.array([T[1], -T[0]]) / np.linalg.norm(T)
+        for t in gll(k - 1):
+            x = (0.5 * (1 - t) * a + 0.5 * (1 + t) * b)[None, :]
+            coeffs.append(par_c[s] * float(grad_u(x)[0] @ n))
+    return np.array(coeffs)
+
+
+def test_poisson_tri_sizes(oracle_mod):
+    form, bucket, nodes, par = poisson_tri(2, 2)
+    i = oracle_mod.OraclePlan(bucket).info
+    assert (i["N"], i["M"], i["n_field"], i["n_trace"], i["n_sides"]) == (39, 24, 9, 15, 3)
+    form, bucket, nodes, par = stokes_tri(1, 2)
+    assert oracle_mod.OraclePlan(bucket).info["N"] == 60  # Stokes VGP tri p=1 (60 ... 295)
+
+
+@pytest.mark.parametrize("k,dk,jitter", [(2, 2, 0.2), (3, 1, 0.15), (4, 2, 0.1)])
+def test_poisson_tri_consistency_linear(oracle_mod, k, dk, jitter):
+    """Triangles: the interpolant of an exact linear solution satisfies B x = F = 0;
+    pins the triangle rule, the lattice basis of the fields, edge parametrisation,
+    normals and parities."""
+    form, bucket, nodes, par = poisson_tri(k, dk, 3, 2, jitter)
+    P = oracle_mod.OraclePlan(bucket)
+    C = nodes.shape[0]
+    G, B, F = P.parts(nodes, par, np.zeros((C, 1, P.info["n_points_total"])))
+    a = np.array([0.7, -1.3])
+    u = lambda X: X @ a + 0.3  # noqa: E731
+    gu = lambda X: np.tile(a, (X.shape[0], 1))  # noqa: E731
+    for c in range(C):
+        x = _tri_trial_interpolant(oracle_mod, nodes[c], par[c], u, gu, k)
+        r = B[c].T @ x
+        assert np.abs(r).max() < 1e-12 * max(1.0, np.abs(B[c]).max()), (c, np.abs(r).max())
+
+
+def test_tri_mesh_parities():
+    nodes, par = mesh.tri_grid(2, 1)
+    # quad 0 holds cells 0 = (v00, v10, v11) and 1 = (v00, v11, v01); they share the
+    # diagonal: side 2 of cell 0 and side 0 of cell 1
+    assert par[0, 2] == 1 and par[1, 0] == -1
+    # side 1 of cell 1 (v11 -> v01) lies on the top boundary
+    assert par[1, 1] == 1
+    # the edge x = h joins cell 0 (side 1, v10 -> v11) and cell 3 (side 2, v01 -> v00 of quad 1)
+    assert par[0, 1] == 1 and par[3, 2] == -1
+    # counter-clockwise vertices: positive signed areas
+    e1, e2 = nodes[:, 1] - nodes[:, 0], nodes[:, 2] - nodes[:, 0]
+    assert (e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0] > 0).all()

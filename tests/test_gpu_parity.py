@@ -13,7 +13,7 @@ torch = pytest.importorskip("torch")
 
 from camellia2_b200 import abi, lib as dlib, mesh  # noqa: E402
 from tests.conftest import rel_fro  # noqa: E402
-from tests.helpers import cdr2d, coeffs_for, poisson2d, poisson3d  # noqa: E402
+from tests.helpers import cdr2d, coeffs_for, poisson2d, poisson3d, poisson_tri, stokes2d, stokes_tri  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -24,6 +24,12 @@ CASES = {
     "poisson3d_k2_dk1": lambda: poisson3d(2, 1, 2, 0.1),          # c5 shapes (N=172, M=110)
     "poisson2d_k1_dk1": lambda: poisson2d(1, 1, 2, 2, 0.1),       # smallest bucket
     "poisson3d_k1_dk2": lambda: poisson3d(1, 2, 2, 0.1),
+    "stokes2d_k1_dk2": lambda: stokes2d(1, 2, 2, 2, 0.1),         # c3 quad p=1 (N=96, M=31)
+    "stokes2d_k2_dk2": lambda: stokes2d(2, 2, 2, 1, 0.1),         # c3 quad p=2 (N=155, M=68)
+    "poisson_tri_k2_dk2": lambda: poisson_tri(2, 2, 2, 2, 0.15),  # triangles (N=39, M=24)
+    "poisson_tri_k4_dk2": lambda: poisson_tri(4, 2, 2, 1, 0.15),
+    "stokes_tri_k1_dk2": lambda: stokes_tri(1, 2, 2, 1, 0.1),     # c3 tri p=1 (N=60)
+    "stokes_tri_k3_dk2": lambda: stokes_tri(3, 2, 1, 1, 0.1),     # c3 tri p=3 (N=133)
 }
 
 
