@@ -1530,12 +1530,105 @@ int dpg_assemble_adjoint(dpg_plan* p, int C, const double* nodes, const int8_t* 
   return dpg_launch_adjoint(&g, &L, (cudaStream_t)stream);
 }
 
-int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags) {
+// Validated per-bucket launch arguments of a multi-bucket call.
+static int multi_args(int n_buckets, const dpg_bucket_batch* buckets, int flags, std::vector<DpgPlanDev>& plans,
+                      std::vector<DpgLaunch>& ls) {
+  if (n_buckets < 0 || (n_buckets > 0 && !buckets)) return fail(DPG_ERR_INVALID_ARGUMENT, "bad bucket list");
   for (int i = 0; i < n_buckets; i++) {
     const dpg_bucket_batch& b = buckets[i];
-    int rc = dpg_assemble(b.plan, b.C, b.nodes, b.parity, b.coeff, b.K, b.l, b.S, b.s, b.info, stream, flags);
-    if (rc != DPG_OK) return rc;
+    if (!b.plan) return fail(DPG_ERR_BAD_PLAN, "null plan in bucket list");
+    if (b.C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+    if (b.C == 0) continue;
+    const DpgPlanDev& g = b.plan->hp.dev;
+    if (!b.nodes || !b.parity || !b.info) return fail(DPG_ERR_INVALID_ARGUMENT, "nodes, parity and info are required");
+    if (g.nslots > 0 && !b.coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+    if (!(flags & DPG_FLAG_NO_K) && (!b.K || !b.l)) return fail(DPG_ERR_INVALID_ARGUMENT, "K and l required");
+    if (!(flags & DPG_FLAG_NO_CONDENSE) && (!b.S || !b.s)) return fail(DPG_ERR_INVALID_ARGUMENT, "S and s required");
+    DpgLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.C = b.C; L.nodes = b.nodes; L.parity = b.parity; L.coeff = b.coeff;
+    L.K = (flags & DPG_FLAG_NO_K) ? nullptr : b.K;
+    L.l = (flags & DPG_FLAG_NO_K) ? nullptr : b.l;
+    L.S = (flags & DPG_FLAG_NO_CONDENSE) ? nullptr : b.S;
+    L.s = (flags & DPG_FLAG_NO_CONDENSE) ? nullptr : b.s;
+    L.info = b.info;
+    plans.push_back(g);
+    ls.push_back(L);
   }
+  return DPG_OK;
+}
+
+int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags) {
+  std::vector<DpgPlanDev> plans;
+  std::vector<DpgLaunch> ls;
+  int rc = multi_args(n_buckets, buckets, flags, plans, ls);
+  if (rc != DPG_OK || plans.empty()) return rc;
+  return dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), (cudaStream_t)stream, nullptr);
+}
+
+struct dpg_graph {
+  DpgMultiDev dev;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+int dpg_graph_capture(int n_buckets, const dpg_bucket_batch* buckets, int flags, dpg_graph** out) {
+  if (!out) return fail(DPG_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  std::vector<DpgPlanDev> plans;
+  std::vector<DpgLaunch> ls;
+  int rc = multi_args(n_buckets, buckets, flags, plans, ls);
+  if (rc != DPG_OK) return rc;
+  if (plans.empty()) return fail(DPG_ERR_INVALID_ARGUMENT, "no cells to capture");
+  dpg_graph* G = new dpg_graph();
+  std::memset(&G->dev, 0, sizeof(G->dev));
+  cudaGetDevice(&G->device);
+  G->dev.bytes = dpg_multi_bytes(plans.data(), ls.data(), (int)plans.size());
+  if (cudaMalloc(&G->dev.base, G->dev.bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete G;
+    return fail(DPG_ERR_OUT_OF_MEMORY, "graph workspace");
+  }
+  rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), nullptr, &G->dev);
+  cudaStream_t cs = nullptr;
+  if (rc == DPG_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+    rc = fail(DPG_ERR_CUDA, "stream creation");
+  if (rc == DPG_OK) {
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      rc = dpg_launch_multi_prepared(&G->dev, cs);
+      cudaError_t e2 = cudaStreamEndCapture(cs, &G->graph);
+      if (rc == DPG_OK && e2 != cudaSuccess) rc = fail(DPG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e2));
+    } else {
+      rc = fail(DPG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    }
+  }
+  if (rc == DPG_OK && cudaGraphInstantiate(&G->exec, G->graph, 0) != cudaSuccess)
+    rc = fail(DPG_ERR_CUDA, "graph instantiation");
+  if (cs) cudaStreamDestroy(cs);
+  if (rc != DPG_OK) {
+    cudaGetLastError();
+    dpg_graph_destroy(G);
+    return rc;
+  }
+  *out = G;
+  return DPG_OK;
+}
+
+int dpg_graph_launch(dpg_graph* G, void* stream) {
+  if (!G || !G->exec) return fail(DPG_ERR_INVALID_ARGUMENT, "null graph");
+  cudaError_t e = cudaGraphLaunch(G->exec, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(DPG_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
+int dpg_graph_destroy(dpg_graph* G) {
+  if (!G) return DPG_OK;
+  if (G->exec) cudaGraphExecDestroy(G->exec);
+  if (G->graph) cudaGraphDestroy(G->graph);
+  if (G->dev.base) cudaFree(G->dev.base);
+  delete G;
   return DPG_OK;
 }
 

@@ -49,3 +49,18 @@ int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d
 int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
+
+// Device tables of a prepared multi-bucket launch (CUDA graph capture).
+struct DpgMultiDev {
+  void* base;          // caller-owned device block: tables, then scratch
+  size_t bytes;
+  DpgPlanDev* plans;
+  DpgLaunch* launches;
+  int* cstart;
+  int nb, grid;
+  void* kernel;
+  size_t smem;
+};
+int dpg_launch_multi(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb, cudaStream_t stream, DpgMultiDev* dev);
+int dpg_launch_multi_prepared(const DpgMultiDev* dev, cudaStream_t stream);
+size_t dpg_multi_bytes(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb);

@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 // The CTA's dynamic shared memory; every shared pointer below is derived from it
 // so the compiler keeps shared-space (LDS/STS) addressing inside the phase functions.
@@ -1079,6 +1080,112 @@ static KernelFn pick_kernel(const DpgPlanDev* plan) {
 
 #include "dpg_adjoint.cuh"
 
+__device__ __forceinline__ void mbar_inval(uint64_t* b) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+// Per-CTA tables of one plan: triangular tile index, G block list, mbarriers.
+__device__ __forceinline__ void cta_setup(const DpgPlanDev& P) {
+  const int tid = threadIdx.x;
+  double* const sm = dpg_smem;
+  int* tri_s = reinterpret_cast<int*>(sm + P.sm_nodes + 32);
+  DpgGTile* tiles_s = reinterpret_cast<DpgGTile*>(sm + P.sm_tiles);
+  uint64_t* mbar_s = reinterpret_cast<uint64_t*>(sm + P.sm_nodes + 26);
+  const int ntri = DPG_MAX_NBT * (DPG_MAX_NBT + 1) / 2;
+  for (int u = tid; u < ntri; u += NT) {
+    int I = (int)((sqrt(8.0 * u + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= u) I++;
+    while (I * (I + 1) / 2 > u) I--;
+    tri_s[u] = I | ((u - I * (I + 1) / 2) << 8);
+  }
+  for (int u = tid; u < P.ngb; u += NT) tiles_s[u] = P.gtiles[u];
+  if (tid == 0) {
+    for (int i = 0; i < 4; i++) mbar_init(&mbar_s[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// Several buckets in one persistent launch.  Work item i of the concatenated cell
+// ranges (bucket b owns [cstart[b], cstart[b+1])) goes to CTA i mod grid, so every
+// CTA walks the buckets in order and switches tables at most nb - 1 times.  The
+// plans live in global memory; their scratch strides are the launch's common one.
+template <int NBTM, int GTM, int BTW>
+__global__ void __launch_bounds__(NT, 1) dpg_multi_kernel(const DpgPlanDev* __restrict__ plans,
+                                                          const DpgLaunch* __restrict__ launches,
+                                                          const int* __restrict__ cstart, int nb) {
+  const int tid = threadIdx.x;
+  Ctx X;
+  uint32_t phase[4] = {0, 0, 0, 0};
+  X.phase = phase;
+  double* const sm = dpg_smem;
+  int cur = -1;
+  const int total = cstart[nb];
+  for (int i = blockIdx.x; i < total; i += gridDim.x) {
+    int b = cur < 0 ? 0 : cur;
+    while (i >= cstart[b + 1]) b++;
+    const DpgPlanDev& P = plans[b];
+    const DpgLaunch& L = launches[b];
+    if (b != cur) {
+      __syncthreads();
+      if (cur >= 0 && tid == 0) {
+        uint64_t* old = reinterpret_cast<uint64_t*>(sm + plans[cur].sm_nodes + 26);
+        for (int k = 0; k < 4; k++) mbar_inval(&old[k]);
+      }
+      __syncthreads();
+      cta_setup(P);
+      for (int k = 0; k < 4; k++) phase[k] = 0;
+      cur = b;
+    }
+    const int cell = i - cstart[b];
+    double* nodes_s = sm + P.sm_nodes;
+    int* flag_s = reinterpret_cast<int*>(sm + P.sm_nodes + 24);
+    double* coef_s = sm + P.sm_coef;
+    if (tid == 0) { flag_s[0] = 0; flag_s[1] = 0; flag_s[2] = 0; }
+    if (tid < P.nv * P.d) nodes_s[tid] = L.nodes[(size_t)cell * P.nv * P.d + tid];
+    const int nco = P.nslots * P.Ptot;
+    if (L.coeff)
+      for (int k = tid; k < nco; k += NT) coef_s[k] = L.coeff[(size_t)cell * nco + k];
+    __syncthreads();
+    phase_b<BTW>(P, L, cell, X);
+    __syncthreads();
+    phase_gram<GTM>(P, L, cell, X);
+    phase_factor(P, X);
+    phase_trsm<NBTM>(P, L, cell, X);
+    phase_syrk_out(P, L, cell, X);
+    __syncthreads();
+    if (tid == 0 && L.info) {
+      int v = 0;
+      if (flag_s[2]) v = ERR_TIMEOUT_FLAG;
+      else if (flag_s[0] != 0) {
+        int r = flag_s[0] - 1;
+        int u = P.dev2user_test[r];
+        v = (u >= 0 ? u : r) + 1;
+      } else if (flag_s[1] != 0) v = flag_s[1];
+      L.info[cell] = v;
+    }
+    __syncthreads();
+  }
+}
+
+typedef void (*MultiFn)(const DpgPlanDev*, const DpgLaunch*, const int*, int);
+#define DPG_MULTI_INSTANCES(X) X(16, 6, 4) X(24, 12, 6)
+
+static MultiFn pick_multi_kernel(const DpgPlanDev* plans, int nb) {
+  int nbt = 0, per = 0, btw = 0;
+  for (int b = 0; b < nb; b++) {
+    const DpgPlanDev* p = &plans[b];
+    nbt = std::max(nbt, p->NBT);
+    per = std::max(per, (p->ngb + DPG_NWARPS - 1) / DPG_NWARPS);
+    for (int s = 0; s < p->nseg; s++) btw = std::max(btw, (p->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
+  }
+#define DPG_PICK(NB, GT, BT) \
+  if (nbt <= NB && per <= GT && btw <= BT) return dpg_multi_kernel<NB, GT, BT>;
+  DPG_MULTI_INSTANCES(DPG_PICK)
+#undef DPG_PICK
+  return nullptr;
+}
+
 static int g_num_sms = 0;
 
 }  // namespace
@@ -1086,7 +1193,14 @@ static int g_num_sms = 0;
 int dpg_configure_kernels(const DpgPlanDev* plan) {
   KernelFn k = pick_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
+  // Several plans may share a kernel instance: the opt-in limit is the device's
+  // maximum, so configuring one plan never lowers another's.
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   size_t bytes = (size_t)plan->sm_total * sizeof(double);
+  if (optin > 0 && bytes > (size_t)optin) return dpg::fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
+  if (optin > 0) bytes = (size_t)optin;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   if (plan->adj_ok) {
@@ -1098,8 +1212,6 @@ int dpg_configure_kernels(const DpgPlanDev* plan) {
     }
   }
   if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (g_num_sms <= 0) g_num_sms = 1;
     // keep freed stream-ordered scratch in the pool between calls
@@ -1160,6 +1272,89 @@ int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_
   cudaFreeAsync(scratch, stream);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
+}
+
+// hplans: host copies of the buckets' plans (their scratch_per_cta is replaced by
+// the common stride here); hl: per-bucket launch arguments; dev: where the device
+// copies of the tables go (null: stream-ordered temporaries freed after the launch).
+int dpg_launch_multi(const DpgPlanDev* hplans_in, const DpgLaunch* hl_in, int nb, cudaStream_t stream,
+                     DpgMultiDev* dev) {
+  std::vector<DpgPlanDev> hplans(hplans_in, hplans_in + nb);
+  std::vector<DpgLaunch> hl(hl_in, hl_in + nb);
+  std::vector<int> cstart(nb + 1, 0);
+  size_t stride = 0, smem = 0;
+  for (int b = 0; b < nb; b++) {
+    cstart[b + 1] = cstart[b] + std::max(0, hl[b].C);
+    stride = std::max(stride, hplans[b].scratch_per_cta);
+    smem = std::max(smem, (size_t)hplans[b].sm_total * sizeof(double));
+  }
+  const int total = cstart[nb];
+  if (total == 0) return DPG_OK;
+  MultiFn k = pick_multi_kernel(hplans.data(), nb);
+  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no multi-bucket kernel instance covers these buckets");
+  int dev_id = 0, optin = 0;
+  cudaGetDevice(&dev_id);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev_id);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin > 0 ? optin : (int)smem);
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  const int grid = std::min(total, g_num_sms > 0 ? g_num_sms : 148);
+  for (auto& p : hplans) p.scratch_per_cta = stride;
+  const size_t bytes_tables = nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)) + (nb + 1) * sizeof(int) + 256;
+  const size_t bytes_scratch = (size_t)grid * stride * sizeof(double);
+  char* base = nullptr;
+  if (dev) {
+    if (dev->bytes < bytes_tables + bytes_scratch) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "multi workspace too small");
+    base = (char*)dev->base;
+  } else {
+    e = cudaMallocAsync((void**)&base, bytes_tables + bytes_scratch, stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("multi workspace: ") + cudaGetErrorString(e));
+    }
+  }
+  double* scratch = (double*)(base + ((bytes_tables + 255) & ~(size_t)255));
+  for (auto& l : hl) l.scratch = scratch;
+  DpgPlanDev* d_plans = (DpgPlanDev*)base;
+  DpgLaunch* d_l = (DpgLaunch*)(base + nb * sizeof(DpgPlanDev));
+  int* d_cs = (int*)(base + nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)));
+  if (dev) {  // outside any capture: synchronous uploads
+    cudaMemcpy(d_plans, hplans.data(), nb * sizeof(DpgPlanDev), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_l, hl.data(), nb * sizeof(DpgLaunch), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_cs, cstart.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    dev->plans = d_plans; dev->launches = d_l; dev->cstart = d_cs; dev->nb = nb; dev->grid = grid;
+    dev->kernel = (void*)k; dev->smem = smem;
+    return DPG_OK;
+  }
+  cudaMemcpyAsync(d_plans, hplans.data(), nb * sizeof(DpgPlanDev), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_l, hl.data(), nb * sizeof(DpgLaunch), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_cs, cstart.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, stream);
+  k<<<grid, NT, smem, stream>>>(d_plans, d_l, d_cs, nb);
+  e = cudaGetLastError();
+  cudaFreeAsync(base, stream);
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
+// Launch of tables prepared by dpg_launch_multi(..., dev) (graph capture records this).
+int dpg_launch_multi_prepared(const DpgMultiDev* dev, cudaStream_t stream) {
+  MultiFn k = (MultiFn)dev->kernel;
+  k<<<dev->grid, NT, dev->smem, stream>>>(dev->plans, dev->launches, dev->cstart, dev->nb);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
+// Bytes a prepared multi-bucket launch needs (tables + scratch).
+size_t dpg_multi_bytes(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb) {
+  size_t stride = 0;
+  int total = 0;
+  for (int b = 0; b < nb; b++) {
+    stride = std::max(stride, hplans[b].scratch_per_cta);
+    total += std::max(0, hl[b].C);
+  }
+  const int grid = std::min(std::max(total, 1), g_num_sms > 0 ? g_num_sms : 148);
+  const size_t tables = nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)) + (nb + 1) * sizeof(int) + 256;
+  return ((tables + 255) & ~(size_t)255) + (size_t)grid * stride * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------

@@ -52,6 +52,9 @@ def load():
     L.dpg_factored_cholesky_solve.argtypes = [i, i, i] + [vp] * 6 + [vp]
     L.dpg_assemble_adjoint.argtypes = [vp, i] + [vp] * 7 + [vp]
     L.dpg_assemble_multi.argtypes = [i, vp, vp, i]
+    L.dpg_graph_capture.argtypes = [i, vp, i, ct.POINTER(vp)]
+    L.dpg_graph_launch.argtypes = [vp, vp]
+    L.dpg_graph_destroy.argtypes = [vp]
     L.dpg_last_error_string.restype = ct.c_char_p
     L.dpg_version.restype = ct.c_char_p
     _LIB = L
@@ -180,3 +183,54 @@ def factoredCholeskySolve(G, B, F, stream=None):
                                               _ptr(F.contiguous()), _ptr(K), _ptr(l), _ptr(info),
                                               _stream_ptr(stream)))
     return K, l, info
+
+
+class BucketBatch(ct.Structure):
+    """dpg_bucket_batch: one bucket's cells and buffers in a multi-bucket call."""
+    _fields_ = [("plan", ct.c_void_p), ("C", ct.c_int)] + [(n, ct.c_void_p) for n in
+                                                           ("nodes", "parity", "coeff", "K", "l", "S", "s", "info")]
+
+
+def _batches(items):
+    """items: list of (Plan, nodes, parity, coeff, out) with device tensors."""
+    arr = (BucketBatch * len(items))()
+    for k, (plan, nodes, parity, coeff, out) in enumerate(items):
+        b = arr[k]
+        b.plan = plan.h.value if hasattr(plan.h, "value") else plan.h
+        b.C = nodes.shape[0]
+        for name, t in (("nodes", nodes), ("parity", parity), ("coeff", coeff), ("K", out["K"]), ("l", out["l"]),
+                        ("S", out["S"]), ("s", out["s"]), ("info", out["info"])):
+            setattr(b, name, None if t is None else t.data_ptr())
+    return arr
+
+
+def assemble_multi(items, stream=None, flags=0):
+    """dpg_assemble_multi: several buckets in one persistent launch."""
+    arr = _batches(items)
+    _check(load().dpg_assemble_multi(len(items), ct.cast(arr, ct.c_void_p), _stream_ptr(stream), flags))
+
+
+class Graph:
+    """dpg_graph_capture / dpg_graph_launch: a captured multi-bucket launch replayed on
+    the buffers named at capture time."""
+
+    def __init__(self, items, flags=0):
+        self._keep = items  # the buffers must outlive the graph
+        arr = _batches(items)
+        h = ct.c_void_p()
+        _check(load().dpg_graph_capture(len(items), ct.cast(arr, ct.c_void_p), flags, ct.byref(h)))
+        self.h = h
+
+    def launch(self, stream=None):
+        _check(load().dpg_graph_launch(self.h, _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().dpg_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

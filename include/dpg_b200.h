@@ -219,8 +219,10 @@ int dpg_assemble_adjoint(dpg_plan* plan, int C, const double* nodes, const int8_
                          const double* coeff, const double* Kbar, const double* lbar,
                          double* coeff_bar, int32_t* info, void* stream);
 
-/* Multi-bucket assembly: one persistent launch walks a work queue over
- * several plans' cell ranges. Pointers per bucket as in dpg_assemble. */
+/* Multi-bucket assembly (TSolution::populateStiffnessAndLoad's loop over
+ * ElementType buckets, Solution.cpp:1131-1297): one persistent launch walks the
+ * concatenated cell ranges of several plans. Pointers per bucket as in
+ * dpg_assemble (device memory). */
 typedef struct dpg_bucket_batch {
   dpg_plan* plan;
   int C;
@@ -235,6 +237,17 @@ typedef struct dpg_bucket_batch {
 } dpg_bucket_batch;
 
 int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags);
+
+/* The same multi-bucket launch recorded once in a CUDA graph and replayed:
+ * for a fixed mesh re-assembled every step (new coefficients written into the
+ * same buffers).  Capture uploads the bucket tables and allocates the
+ * workspace (outside any stream capture of the caller); every launch then
+ * reads the buffers named at capture time.  Launches of one graph must not
+ * overlap on the GPU (they share the workspace). */
+typedef struct dpg_graph dpg_graph;
+int dpg_graph_capture(int n_buckets, const dpg_bucket_batch* buckets, int flags, dpg_graph** out);
+int dpg_graph_launch(dpg_graph* graph, void* stream);
+int dpg_graph_destroy(dpg_graph* graph);
 
 /* dpg_assemble without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory while
