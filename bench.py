@@ -304,14 +304,19 @@ def main():
             except Exception:
                 traffic = None
         cpu = None if args.no_cpu else cpu_baseline(bucket, nodes, par, coeff)
+        M_, t_ = info["M"], info["n_trace"]
+        out_bytes = 8 * C * (M_ * M_ + M_ + t_ * t_ + t_) + 4 * C
+        in_bytes = C * (8 * info["n_vertices"] * info["space_dim"] + info["n_sides"] +
+                        8 * info["n_slots"] * info["n_points_total"])
         line = {
             "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"3D hex Poisson ultraweak DPG, {n}^3 jittered hexes (0.1h), k=2 dk=1 "
                                    f"(N={info['N']}, M={info['M']}, f={info['n_field']}, t={info['n_trace']})",
-                       "cells": C, "form": "fp64", "l2": "no flush: each step reads 0.15 GB and writes 16.3 GB "
-                                                          "(> 126 MB L2)",
+                       "cells": C, "form": "fp64",
+                       "l2": f"no flush: each step reads {in_bytes / 1e9:.2f} GB and writes {out_bytes / 1e9:.1f} GB "
+                             f"({'>' if out_bytes > 126e6 else '<'} 126 MB L2)",
                        "parallelism": f"{world} GPU(s), cells sharded (weak), no data-path collective"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
