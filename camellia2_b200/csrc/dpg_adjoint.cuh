@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_adjoint_kernel(const __grid_constan
     __syncthreads();
     phase_b<BTW>(P, L, cell, X);
     __syncthreads();
-    phase_gram<GTM>(P, L, cell, X);
+    phase_gram<GTM, 0>(P, L, cell, X);
     phase_factor(P, X);
     phase_adj_solve<NBTM>(P, L);
     phase_adj_p<NBTM>(P, L, cell);

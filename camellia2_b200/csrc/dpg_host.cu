@@ -1292,6 +1292,7 @@ int dpg_make_solve_plan(int N, int M, DpgPlanDev* out) {
   g.sm_tiles = g.sm_coef;
   g.sm_nodes = g.sm_tiles;
   g.scratch_per_cta = 0;
+  g.chg = DPG_CHG;  // no Gram phase; selects the standard kernel instances
   g.sm_invd = g.sm_nodes + 192;
   g.sm_total = g.sm_invd + al(std::max(g.Np, g.Mp));
   return DPG_OK;

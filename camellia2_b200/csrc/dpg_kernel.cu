@@ -594,10 +594,83 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
   }
 }
 
+// The Gram chunk loop for CH points per chunk (compile-time, so the h and DMMA loops
+// unroll completely).
+template <int GTM, int CH>
+__device__ __forceinline__ void gram_chunks(const DpgPlanDev& P, const Ctx& X, const double* Dm, double* hb, int nunit,
+                                            int ntw, const uint32_t (&pk)[GTM], double (&acc)[GTM][4]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  DPG_SMEM_VIEWS(P);
+  const int nch = P.QGpad / CH;
+  const uint32_t chunk_bytes = (uint32_t)(CH * P.featstride * sizeof(double));
+  for (int c = 0; c < nch; c++) {
+    const int buf = c & 1;
+    const double* fref = sm + (buf ? P.g_fref1 : P.g_fref0);
+    if (tid == 0) {
+      if (c + 1 < nch) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&mbar_s[buf ^ 1], chunk_bytes);
+        bulk_g2s(sm + (buf ? P.g_fref0 : P.g_fref1), P.frefG + (size_t)(c + 1) * CH * P.featstride,
+                 chunk_bytes, &mbar_s[buf ^ 1]);
+      }
+      if (!mbar_wait(&mbar_s[buf], X.phase[buf] & 1)) flag_s[2] = 1;
+    }
+    X.phase[buf]++;
+    __syncthreads();
+    // h_{b->a}[q] = D_q (4x4, padded to 8 rows) * slots_b[q] (4 x 8 column tile): one DMMA per unit and point
+    for (int un = warp; un < nunit; un += DPG_NWARPS) {
+      int r = un, p = 0;
+      while (r >= P.test[P.pair_b[p]].ntiles) { r -= P.test[P.pair_b[p]].ntiles; p++; }
+      const int b = P.pair_b[p];
+      const int ld = P.test[b].ldA;
+      const double* dp = Dm + ((size_t)c * CH * P.npairs + p) * 16 + g * 4 + t;
+      const double* fp = fref + P.test[b].foff + t * ld + r * 8 + g;
+      double* hp = hb + P.hoff[p] + g * ld + r * 8 + 2 * t;
+#pragma unroll
+      for (int lq = 0; lq < CH; lq++) {
+        const double av = (g < 4) ? dp[lq * P.npairs * 16] : 0.0;
+        const double bv = fp[lq * P.featstride];
+        double2 hc = make_double2(0.0, 0.0);
+        dmma(hc, av, bv);
+        if (g < 4) *reinterpret_cast<double2*>(hp + lq * P.hstride) = hc;
+      }
+    }
+    __syncthreads();
+    // m16n8k16 over the owned blocks: one k16 step = 4 points x 4 slots
+#pragma unroll 1
+    for (int s4 = 0; s4 < CH; s4 += 4) {
+      const double* fa = fref + s4 * P.featstride;
+      const double* hq = hb + s4 * P.hstride;
+      uint32_t prevA = 0xffffffffu;
+      double av[8];
+#pragma unroll
+      for (int u = 0; u < GTM; u++) {
+        if (u < ntw) {
+          const uint32_t ao = pk[u] & 0xffffu, bo = pk[u] >> 16;
+          if (ao != prevA) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              av[2 * i] = fa[i * P.featstride + ao];
+              av[2 * i + 1] = fa[i * P.featstride + ao + 8];
+            }
+            prevA = ao;
+          }
+          double bv[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) bv[i] = hq[i * P.hstride + bo];
+          dmma16(acc[u], av, bv);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Phase 2: Gram matrix -> lower tiles in shared memory
 // ---------------------------------------------------------------------------
-template <int GTM>
+template <int GTM, int CHG>
 __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch& L, int cell, const Ctx& X) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -607,7 +680,6 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
   double* Dm = sm + P.g_D;  // [q][pair][16]
   double* hb = sm + P.g_h;
   double* GT = sm + P.sm_gt;
-  const int nch = P.QGpad / P.chg;
   const uint32_t chunk_bytes = (uint32_t)(P.chg * P.featstride * sizeof(double));
   if (tid == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -672,67 +744,9 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
   int nunit = 0;
   for (int p = 0; p < P.npairs; p++) nunit += P.test[P.pair_b[p]].ntiles;
   __syncthreads();
-  for (int c = 0; c < nch; c++) {
-    const int buf = c & 1;
-    const double* fref = sm + (buf ? P.g_fref1 : P.g_fref0);
-    if (tid == 0) {
-      if (c + 1 < nch) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&mbar_s[buf ^ 1], chunk_bytes);
-        bulk_g2s(sm + (buf ? P.g_fref0 : P.g_fref1), P.frefG + (size_t)(c + 1) * P.chg * P.featstride,
-                 chunk_bytes, &mbar_s[buf ^ 1]);
-      }
-      if (!mbar_wait(&mbar_s[buf], X.phase[buf] & 1)) flag_s[2] = 1;
-    }
-    X.phase[buf]++;
-    __syncthreads();
-    // h_{b->a}[q] = D_q (4x4, padded to 8 rows) * slots_b[q] (4 x 8 column tile): one DMMA per unit and point
-    for (int un = warp; un < nunit; un += DPG_NWARPS) {
-      int r = un, p = 0;
-      while (r >= P.test[P.pair_b[p]].ntiles) { r -= P.test[P.pair_b[p]].ntiles; p++; }
-      const int b = P.pair_b[p];
-      const int ld = P.test[b].ldA;
-      const double* dp = Dm + ((size_t)c * P.chg * P.npairs + p) * 16 + g * 4 + t;
-      const double* fp = fref + P.test[b].foff + t * ld + r * 8 + g;
-      double* hp = hb + P.hoff[p] + g * ld + r * 8 + 2 * t;
-#pragma unroll 4
-      for (int lq = 0; lq < P.chg; lq++) {
-        const double av = (g < 4) ? dp[lq * P.npairs * 16] : 0.0;
-        const double bv = fp[lq * P.featstride];
-        double2 hc = make_double2(0.0, 0.0);
-        dmma(hc, av, bv);
-        if (g < 4) *reinterpret_cast<double2*>(hp + lq * P.hstride) = hc;
-      }
-    }
-    __syncthreads();
-    // m16n8k16 over the owned blocks: one k16 step = 4 points x 4 slots
-#pragma unroll 1
-    for (int s4 = 0; s4 < P.chg; s4 += 4) {
-      const double* fa = fref + s4 * P.featstride;
-      const double* hq = hb + s4 * P.hstride;
-      uint32_t prevA = 0xffffffffu;
-      double av[8];
-#pragma unroll
-      for (int u = 0; u < GTM; u++) {
-        if (u < ntw) {
-          const uint32_t ao = pk[u] & 0xffffu, bo = pk[u] >> 16;
-          if (ao != prevA) {
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-              av[2 * i] = fa[i * P.featstride + ao];
-              av[2 * i + 1] = fa[i * P.featstride + ao + 8];
-            }
-            prevA = ao;
-          }
-          double bv[4];
-#pragma unroll
-          for (int i = 0; i < 4; i++) bv[i] = hq[i * P.hstride + bo];
-          dmma16(acc[u], av, bv);
-        }
-      }
-    }
-    __syncthreads();
-  }
+  if (CHG != 0) gram_chunks<GTM, CHG != 0 ? CHG : DPG_CHG>(P, X, Dm, hb, nunit, ntw, pk, acc);
+  else if (P.chg == DPG_CHG) gram_chunks<GTM, DPG_CHG>(P, X, Dm, hb, nunit, ntw, pk, acc);
+  else gram_chunks<GTM, DPG_CHG / 2>(P, X, Dm, hb, nunit, ntw, pk, acc);
   // accumulators -> tile-lower shared storage (overlaps the staging area); tiles of
   // uncoupled var pairs are zero
   for (int e = tid; e < P.ngz * 64; e += NT) GT[P.gzero[e >> 6] * 64 + (e & 63)] = 0.0;
@@ -976,7 +990,7 @@ __device__ __forceinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLau
   }
 }
 
-template <int NBTM, int GTM, int BTW>
+template <int NBTM, int GTM, int BTW, int CHG>
 __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
   const int tid = threadIdx.x;
   Ctx X;
@@ -1033,7 +1047,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
     } else {
       phase_b<BTW>(P, L, cell, X);
       __syncthreads();
-      phase_gram<GTM>(P, L, cell, X);
+      phase_gram<GTM, CHG>(P, L, cell, X);
       if (L.parts) {
         __syncthreads();
         continue;
@@ -1061,9 +1075,11 @@ __global__ void __launch_bounds__(NT, 1) dpg_cell_kernel(const __grid_constant__
   }
 }
 
-// Instances: register arrays sized for the test-tile count of the bucket.
+// Instances: register arrays sized for the test-tile count of the bucket; the last
+// argument is the Gram chunk size (plans short of shared memory use half chunks).
 #define DPG_INSTANCES(X) \
-  X(8, 3, 4) X(12, 5, 4) X(16, 6, 4) X(18, 8, 4) X(20, 8, 4) X(22, 9, 3) X(24, 12, 4) X(24, 12, 6)
+  X(8, 3, 4, 8) X(12, 5, 4, 8) X(16, 6, 4, 8) X(18, 8, 4, 8) X(20, 8, 4, 8) X(22, 9, 3, 8) X(24, 12, 4, 8) \
+  X(24, 12, 6, 8) X(24, 12, 6, 4)
 
 typedef void (*KernelFn)(const DpgPlanDev, const DpgLaunch);
 
@@ -1071,8 +1087,8 @@ static KernelFn pick_kernel(const DpgPlanDev* plan) {
   const int per = (plan->ngb + DPG_NWARPS - 1) / DPG_NWARPS;
   int btw = 0;
   for (int s = 0; s < plan->nseg; s++) btw = std::max(btw, (plan->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
-#define DPG_PICK(NB, GT, BT) \
-  if (plan->NBT <= NB && per <= GT && btw <= BT) return dpg_cell_kernel<NB, GT, BT>;
+#define DPG_PICK(NB, GT, BT, CH) \
+  if (plan->NBT <= NB && per <= GT && btw <= BT && plan->chg == CH) return dpg_cell_kernel<NB, GT, BT, CH>;
   DPG_INSTANCES(DPG_PICK)
 #undef DPG_PICK
   return nullptr;
@@ -1149,7 +1165,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_multi_kernel(const DpgPlanDev* __re
     __syncthreads();
     phase_b<BTW>(P, L, cell, X);
     __syncthreads();
-    phase_gram<GTM>(P, L, cell, X);
+    phase_gram<GTM, 0>(P, L, cell, X);
     phase_factor(P, X);
     phase_trsm<NBTM>(P, L, cell, X);
     phase_syrk_out(P, L, cell, X);
