@@ -1122,12 +1122,25 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
         }
       }
     }
+    // entries: (scratch element, first contribution, count, side term of the first |
+    // 1 << 16 when no bilinear block writes the element's column tile, so a store suffices)
+    std::vector<char> blk_col(g.MBT + 1, 0);
+    for (int sg = 0; sg < g.nseg; sg++)
+      for (int kb = 0; kb < g.seg[sg].nblk; kb++) blk_col[g.seg[sg].blk[kb].J] = 1;
     std::vector<int4> sent;
     std::vector<int> scon_se;
+    std::vector<int2> rc;
     std::vector<std::vector<double>> wl;
     for (auto& kv : ent) {
-      sent.push_back(make_int4(kv.first.first, kv.first.second, (int)scon_se.size(), (int)kv.second.size()));
-      for (auto& c : kv.second) { scon_se.push_back(c.first); wl.push_back(c.second); }
+      const int row = kv.first.first, col = kv.first.second;
+      const int idx = (((col >> 3) * g.NBT + (row >> 3)) * 32 + (row & 7) * 4 + ((col & 7) >> 1)) * 2 + (col & 1);
+      const int store = blk_col[col >> 3] ? 0 : 1;
+      sent.push_back(make_int4(idx, (int)scon_se.size(), (int)kv.second.size(), kv.second[0].first | (store << 16)));
+      for (auto& c : kv.second) {
+        scon_se.push_back(c.first);
+        wl.push_back(c.second);
+        rc.push_back(make_int2(row, col));
+      }
     }
     g.nse = (int)ses.size();
     g.nsent = (int)sent.size();
@@ -1150,9 +1163,6 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     g.scon_w = upload(P, wq);
     // reverse mode: contributions grouped by side term, with their (row, col)
     std::vector<int> sstart(g.nse + 1, 0), scon;
-    std::vector<int2> rc(g.ncon);
-    for (size_t e = 0; e < sent.size(); e++)
-      for (int c = sent[e].z; c < sent[e].z + sent[e].w; c++) rc[c] = make_int2(sent[e].x, sent[e].y);
     for (int se = 0; se < g.nse; se++) {
       sstart[se] = (int)scon.size();
       for (int c = 0; c < g.ncon; c++)

@@ -421,14 +421,51 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
   for (int q = tid; q < P.nbpts; q += NT)
     point_geometry(d, nv, nodes_s, P.dNB + (size_t)q * nv * d, P.wB[q], q >= P.QB ? P.tangB + (size_t)q * 6 : nullptr,
                    geo + q * GEO);
+  // separable side terms, while the first volume chunk is in flight: per-point factors,
+  // then one thread per entry (scratch element); entries are unique, and an element
+  // that a bilinear block also writes is read-modified-written (the blocks add to it
+  // after the chunk loop's barriers)
+  if (P.nse > 0) {
+    double* fac = sm + P.b_fac;  // [nse][QS]
+    __syncthreads();             // geometry complete, scratch zeroed
+    for (int task = tid; task < P.nse * P.QS; task += NT) {
+      const int se = task / P.QS, q = task - se * P.QS;
+      const DpgSideTerm& E = P.se[se];
+      const double* gq = geo + (P.QB + E.side * P.QS + q) * GEO;
+      double v = E.coef;
+      if (E.use_meas) v *= gq[19];
+      if (E.slot >= 0) v *= coef_s[E.slot * P.Ptot + E.pbase + q];
+      if (E.normal_comp >= 0) v *= gq[20 + E.normal_comp];
+      if (E.flux) v *= (double)par_c[E.side];
+      fac[task] = v;
+    }
+    __syncthreads();
+    double* scd = reinterpret_cast<double*>(scr);
+    for (int e = tid; e < P.nsent; e += NT) {
+      const int4 en = __ldg(P.sent + e);
+      double acc = 0.0;
+      if (en.z == 1) {
+        const double* f = fac + (en.w & 0xffff) * P.QS;
+        const double* w = P.scon_w + en.y;
+        for (int q = 0; q < P.QS; q++) acc += __ldg(w + (size_t)q * P.ncon) * f[q];
+      } else {
+        for (int c = en.y; c < en.y + en.z; c++) {
+          const double* f = fac + __ldg(P.scon_se + c) * P.QS;
+          for (int q = 0; q < P.QS; q++) acc += __ldg(P.scon_w + (size_t)q * P.ncon + c) * f[q];
+        }
+      }
+      if (en.w >> 16) scd[en.x] = acc;
+      else scd[en.x] += acc;
+    }
+  }
   int gc = 0;  // global chunk counter (buffer parity)
   for (int sgi = first_seg; sgi < P.nseg; sgi++) {
     const DpgSeg& S = P.seg[sgi];
     if (S.nterm == 0) continue;
     // this warp's active 16x8 blocks of the segment: operand offsets and accumulators
-    const int per = (S.ntile + DPG_NWARPS - 1) / DPG_NWARPS;
-    const int my0 = S.tile0 + warp * per;
-    const int nmine = max(0, min(per, S.tile0 + S.ntile - my0));
+    const int bbase = S.ntile / DPG_NWARPS, bextra = S.ntile % DPG_NWARPS;
+    const int my0 = S.tile0 + warp * bbase + min(warp, bextra);
+    const int nmine = bbase + (warp < bextra ? 1 : 0);
     uint32_t pk[BTW];
     double acc[BTW][4];
 #pragma unroll
@@ -542,36 +579,6 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
         scr[s0] = v0;
         scr[s0 + 32] = v1;
       }
-    }
-  }
-  // separable side terms: one thread per entry (row, col); entries are unique, so the
-  // read-modify-write of the scratch element needs no atomics
-  if (P.nse > 0) {
-    double* fac = sm + P.b_fac;  // [nse][QS]
-    __syncthreads();             // segment contributions are in the scratch
-    for (int task = tid; task < P.nse * P.QS; task += NT) {
-      const int se = task / P.QS, q = task - se * P.QS;
-      const DpgSideTerm& E = P.se[se];
-      const double* gq = geo + (P.QB + E.side * P.QS + q) * GEO;
-      double v = E.coef;
-      if (E.use_meas) v *= gq[19];
-      if (E.slot >= 0) v *= coef_s[E.slot * P.Ptot + E.pbase + q];
-      if (E.normal_comp >= 0) v *= gq[20 + E.normal_comp];
-      if (E.flux) v *= (double)par_c[E.side];
-      fac[task] = v;
-    }
-    __syncthreads();
-    double* scd = reinterpret_cast<double*>(scr);
-    for (int e = tid; e < P.nsent; e += NT) {
-      const int4 en = __ldg(P.sent + e);
-      double acc = 0.0;
-      for (int c = en.z; c < en.z + en.w; c++) {
-        const double* f = fac + __ldg(P.scon_se + c) * P.QS;
-        for (int q = 0; q < P.QS; q++) acc += __ldg(P.scon_w + (size_t)q * P.ncon + c) * f[q];
-      }
-      const int r = en.x & 7, cc = en.y & 7;
-      const size_t idx = ((size_t)((en.y >> 3) * P.NBT + (en.x >> 3)) * 32 + r * 4 + (cc >> 1)) * 2 + (cc & 1);
-      scd[idx] += acc;
     }
   }
   if (!L.parts) return;
@@ -723,9 +730,11 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
     Dm[task] = sacc * geo[q * GEO + 19];
   }
   // owned 16x8 blocks: packed per-thread operand offsets (A | B << 16)
-  const int per = (P.ngb + DPG_NWARPS - 1) / DPG_NWARPS;
-  const int tau0 = warp * per;
-  const int ntw = max(0, min(per, P.ngb - tau0));
+  // balanced: warps 0 .. extra-1 take one block more, so the four SM sub-partitions
+  // (warps w, w+4, w+8, w+12) carry equal tensor work
+  const int gbase = P.ngb / DPG_NWARPS, gextra = P.ngb % DPG_NWARPS;
+  const int ntw = gbase + (warp < gextra ? 1 : 0);
+  const int tau0 = warp * gbase + min(warp, gextra);
   const int4* tdesc = reinterpret_cast<const int4*>(sm + P.sm_tiles) + tau0;
   uint32_t pk[GTM];
   double acc[GTM][4];
@@ -923,9 +932,9 @@ __device__ __forceinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLau
   double* KT = sm + P.sm_k;
   {
     const int nk = P.MBT * (P.MBT + 1) / 2;
-    const int per = (nk + DPG_NWARPS - 1) / DPG_NWARPS;
-    const int k0 = warp * per;
-    const int nkw = max(0, min(per, nk - k0));
+    const int kbase = nk / DPG_NWARPS, kextra = nk % DPG_NWARPS;
+    const int k0 = warp * kbase + min(warp, kextra);
+    const int nkw = kbase + (warp < kextra ? 1 : 0);
     double2 kacc[DPG_MAX_KT];
     int kI[DPG_MAX_KT], kJ[DPG_MAX_KT];
 #pragma unroll
@@ -956,20 +965,21 @@ __device__ __forceinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLau
       if (u < nkw) *reinterpret_cast<double2*>(KT + (k0 + u) * 64 + ak_cfrag(g, t)) = kacc[u];
     __syncthreads();
   }
-  // K and l out (user numbering; fields first: dev = i for i < nf, nfp + (i - nf) otherwise)
+  // K and l out (user numbering; fields first: dev = i for i < nf, nfp + (i - nf) otherwise);
+  // streaming stores, so the outputs do not evict the CTA's scratch slot from L2
   if (L.K) {
     double* Kc = L.K + (size_t)cell * P.M * P.M;
     for (int i = warp; i < P.M; i += DPG_NWARPS) {
       const int di = i < P.nf ? i : P.nfp + (i - P.nf);
       for (int j = lane; j < P.M; j += 32) {
         const int dj = j < P.nf ? j : P.nfp + (j - P.nf);
-        Kc[(size_t)i * P.M + j] = sym_get(KT, di, dj);
+        __stcs(&Kc[(size_t)i * P.M + j], sym_get(KT, di, dj));
       }
     }
     double* lc = L.l + (size_t)cell * P.M;
     for (int i = tid; i < P.M; i += NT) {
       int di = i < P.nf ? i : P.nfp + (i - P.nf);
-      lc[i] = sym_get(KT, P.fcol, di);
+      __stcs(&lc[i], sym_get(KT, P.fcol, di));
     }
   }
   if (L.S && P.nt > 0) {
@@ -984,9 +994,9 @@ __device__ __forceinline__ void phase_syrk_out(const DpgPlanDev& P, const DpgLau
     }
     double* Sc = L.S + (size_t)cell * P.nt * P.nt;
     for (int i = warp; i < P.nt; i += DPG_NWARPS)
-      for (int j = lane; j < P.nt; j += 32) Sc[(size_t)i * P.nt + j] = sym_get(KT, P.nfp + i, P.nfp + j);
+      for (int j = lane; j < P.nt; j += 32) __stcs(&Sc[(size_t)i * P.nt + j], sym_get(KT, P.nfp + i, P.nfp + j));
     double* sc = L.s + (size_t)cell * P.nt;
-    for (int i = tid; i < P.nt; i += NT) sc[i] = sym_get(KT, P.fcol, P.nfp + i);
+    for (int i = tid; i < P.nt; i += NT) __stcs(&sc[i], sym_get(KT, P.fcol, P.nfp + i));
   }
 }
 

@@ -169,7 +169,8 @@ struct DpgPlanDev {
   // contributions c of each entry (row, col)
   int nse, nsent, ncon;
   const DpgSideTerm* se;    // [nse]
-  const int4* sent;         // [nsent] (device row, device column, first contribution, count)
+  const int4* sent;         // [nsent] (scratch element, first contribution, count, side term of the
+                            //  first | 1 << 16 when the element has no other writer)
   const int* scon_se;       // [ncon] side term of each contribution
   const double* scon_w;     // [QS][ncon]
   // reverse mode (dpg_assemble_adjoint)
