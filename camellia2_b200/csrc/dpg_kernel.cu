@@ -331,9 +331,9 @@ __device__ __forceinline__ void factor_diag(double* __restrict__ T, int k, int* 
 }
 
 // Blocked right-looking Cholesky of the leading nsteps tiles of a tile-lower
-// matrix with nb tiles in shared memory (AK tiles).  Look-ahead: while warps
-// 1..15 apply the trailing update of step k, warp 0 updates diagonal tile k+1
-// first and factors it, so each step costs two barriers.  The panel multiplies by
+// matrix with nb tiles in shared memory (AK tiles).  Look-ahead: while the warps
+// of sub-partitions 1..3 apply the trailing update of step k, warp 0 updates diagonal
+// tile k+1 first and factors it, so each step costs two barriers.  The panel multiplies by
 // the inverse diagonal tile (two DMMAs per tile).  linv (NBT x 64) receives the
 // inverses of the factored diagonal tiles; invd the inverse pivots.
 __device__ __noinline__ void tile_cholesky(int T_off, int nb, int nsteps, int flag_idx, int sgn, int tri_off,
@@ -376,8 +376,12 @@ __device__ __noinline__ void tile_cholesky(int T_off, int nb, int nsteps, int fl
         __syncwarp();
         if (k + 1 < nsteps) factor_diag(T, k + 1, flag, sgn, invd, linv);
       }
-    } else {
-      for (int u = 1 + (warp - 1); u < ntr; u += DPG_NWARPS - 1) {
+    } else if (warp & 3) {
+      // the update runs on the other three sub-partitions' warps: warps 4, 8, 12 stay
+      // idle so that warp 0's serial diagonal factorisation has its sub-partition (issue
+      // slots) to itself; it is the critical path of every step
+      const int hidx = warp - (warp >> 2) - 1;
+      for (int u = 1 + hidx; u < ntr; u += DPG_NWARPS - DPG_NWARPS / 4) {
         int ij = tri[u];
         int i = k + 1 + (ij & 255), j = k + 1 + (ij >> 8);
         double* Tij = T + (i * (i + 1) / 2 + j) * 64;
