@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--n", type=int, default=48, help="cells per direction (48 -> 110,592 cells)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-extra", action="store_true", help="skip the other configurations' timings")
     return p.parse_args()
 
 
@@ -63,6 +64,72 @@ def build_workload(n, seed):
 def make_coeff(C, P, seed):
     rng = np.random.default_rng(seed + 1000)
     return rng.uniform(-1.0, 1.0, size=(C, 1, P))
+
+
+def other_configs(torch):
+    """Device throughput (CUDA events, inputs resident) of the other configurations the
+    path covers, on seeded synthetic meshes of their sizes: c2 (2D Poisson UW k=4 dk=2,
+    256^2 jittered quads), c4 (2D CDR UW k=3 dk=2, 128^2 quads, forward and reverse
+    mode with J = sum r^T K r + g^T l), and the c3 buckets one CTA holds (Stokes VGP
+    quads p=1,2 and triangles p=1..3, Delta p=2) in one multi-bucket launch.  Context
+    for the headline, not bench lines."""
+    from camellia2_b200 import abi, formulation as fm, lib, mesh
+
+    def timeit(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    dev = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()  # noqa: E731
+    res = {}
+    # c2
+    b = fm.PoissonFormulation(2).bucket(abi.TOPO_QUAD, 4, 2)
+    plan = lib.Plan(b)
+    nodes, par = mesh.quad_grid(256, 256, 0.2, seed=1)
+    C = nodes.shape[0]
+    co = mesh.uniform_coeff(C, 1, plan.info["n_points_total"], seed=1)
+    dn, dp, dc = dev(nodes), dev(par), dev(co)
+    out = plan.alloc_outputs(C)
+    ms = timeit(lambda: plan.assemble(dn, dp, dc, out=out))
+    res["c2_poisson2d_k4_256sq"] = {"cells": C, "ms": ms, "cells_per_s": C / ms * 1e3}
+    del out
+    # c4 forward and reverse
+    b = fm.ConvectionDiffusionReactionFormulation(2).bucket(abi.TOPO_QUAD, 3, 2)
+    plan = lib.Plan(b)
+    nodes, par = mesh.quad_grid(128, 128, 0.1, seed=1)
+    C = nodes.shape[0]
+    co = mesh.cdr_coeff(C, plan.info, seed=1)
+    dn, dp, dc = dev(nodes), dev(par), dev(co)
+    out = plan.alloc_outputs(C)
+    ms = timeit(lambda: plan.assemble(dn, dp, dc, out=out))
+    res["c4_cdr2d_k3_128sq"] = {"cells": C, "ms": ms, "cells_per_s": C / ms * 1e3}
+    M = plan.info["M"]
+    rng = np.random.default_rng(5)
+    r = rng.normal(size=(C, M))
+    Kbar, lbar = dev(r[:, :, None] * r[:, None, :]), dev(rng.normal(size=(C, M)))
+    ms = timeit(lambda: plan.adjoint(dn, dp, dc, Kbar, lbar))
+    res["c4_cdr2d_k3_128sq_adjoint"] = {"cells": C, "ms": ms, "cells_per_s": C / ms * 1e3}
+    del out, Kbar
+    # c3 buckets that fit one CTA, one multi-bucket launch
+    items, total = [], 0
+    for topo, k, make in ((abi.TOPO_QUAD, 1, mesh.quad_grid), (abi.TOPO_QUAD, 2, mesh.quad_grid),
+                          (abi.TOPO_TRI, 1, mesh.tri_grid), (abi.TOPO_TRI, 2, mesh.tri_grid),
+                          (abi.TOPO_TRI, 3, mesh.tri_grid)):
+        pl = lib.Plan(fm.StokesVGPFormulation(2).bucket(topo, k, 2))
+        nodes, par = make(64, 64 if topo == abi.TOPO_QUAD else 32, 0.1, seed=k)
+        C = nodes.shape[0]
+        co = mesh.uniform_coeff(C, pl.info["n_slots"], pl.info["n_points_total"], seed=k)
+        items.append((pl, dev(nodes), dev(par), dev(co), pl.alloc_outputs(C)))
+        total += C
+    ms = timeit(lambda: lib.assemble_multi(items))
+    res["c3_stokes_quads_p1_2_tris_p1_3_multi"] = {"cells": total, "ms": ms, "cells_per_s": total / ms * 1e3}
+    return res
 
 
 class ClockSampler:
@@ -327,6 +394,7 @@ def main():
             "clocks": clocks,
             "parity_vs_oracle_max_rel": parity,
             "info_nonzero_cells": bad,
+            "other_configs": None if args.no_extra else other_configs(torch),
         }
         print(json.dumps(line), flush=True)
     if world > 1:
