@@ -271,6 +271,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from camellia2_b200 import lib
+    from camellia2_b200.shard import max_over_ranks
 
     n = args.n
     bucket, nodes, par = build_workload(n, 1 + rank)
@@ -315,11 +316,7 @@ def main():
     if world > 1:
         dist.barrier()
     clocks = clk.stop()
-    ms_total = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dev)
     ms = ms_total / args.steps
     value = world * C / (ms * 1e-3)
     bad = int((out["info"] != 0).sum().item())
@@ -347,11 +344,7 @@ def main():
             plan.assemble_host(h_nodes, h_par, h_co, out=hout)
         f1.record(stream)
         torch.cuda.synchronize()
-        ems = f0.elapsed_time(f1) / e_steps
-        if world > 1:
-            tt = torch.tensor([ems], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ems = float(tt.item())
+        ems = max_over_ranks(f0.elapsed_time(f1) / e_steps, dev)
         h2d = sum(x.numel() * x.element_size() for x in (h_nodes, h_par, h_co))
         d2h = sum(x.numel() * x.element_size() for x in hout.values())
         e2e = {"value": world * C / (ems * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": h2d,
