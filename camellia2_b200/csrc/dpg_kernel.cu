@@ -89,8 +89,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 
 // Bounded wait on an mbarrier phase; false if the limit was reached.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
-  for (int it = 0; it < MBAR_SPIN_LIMIT; it++) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int limit = MBAR_SPIN_LIMIT) {
+  for (int it = 0; it < limit; it++) {
     uint32_t done;
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -1276,6 +1276,30 @@ int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const 
   k<<<grid, NT, bytes, stream>>>(*plan, L);
   cudaError_t e = cudaGetLastError();
   if (scratch) cudaFreeAsync(scratch, stream);
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
+// Bounded-wait probe: one thread waits, with the kernels' own wait routine, on an
+// mbarrier whose transaction never arrives (a flag nothing sets), and reports the
+// status the assembly kernels turn into info = 0x7fff0000.  Lets a test check that a
+// stalled staging copy ends the wait with an error instead of hanging the GPU.
+namespace {
+__global__ void wait_probe_kernel(int limit, int* status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_expect_tx(&bar, 16);  // no copy will deliver these bytes
+    status[0] = mbar_wait(&bar, 0, limit) ? 0 : ERR_TIMEOUT_FLAG;
+  }
+}
+}  // namespace
+
+extern "C" int dpg_debug_wait_probe(int limit, int* status_dev, void* stream) {
+  if (limit <= 0 || !status_dev) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  wait_probe_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(limit, status_dev);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
 }
