@@ -1569,6 +1569,17 @@ static int multi_args(int n_buckets, const dpg_bucket_batch* buckets, int flags,
   return DPG_OK;
 }
 
+int dpg_recover_fields(dpg_plan* p, int C, const double* K, const double* l, const double* trace_coeff,
+                       double* local_coeff, int32_t* info, void* stream) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!K || !l || !local_coeff || !info || (p->hp.dev.nt > 0 && !trace_coeff))
+    return fail(DPG_ERR_INVALID_ARGUMENT, "K, l, trace coefficients, output and info are required");
+  const DpgPlanDev& g = p->hp.dev;
+  return dpg_launch_recover_fields(C, g.M, g.nf, K, l, trace_coeff, local_coeff, info, (cudaStream_t)stream);
+}
+
 int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags) {
   std::vector<DpgPlanDev> plans;
   std::vector<DpgLaunch> ls;

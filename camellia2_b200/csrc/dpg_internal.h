@@ -49,6 +49,8 @@ int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d
 int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
+int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const double* l, const double* t, double* u,
+                              int32_t* info, cudaStream_t stream);
 
 // Device tables of a prepared multi-bucket launch (CUDA graph capture).
 struct DpgMultiDev {

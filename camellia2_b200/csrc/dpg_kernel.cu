@@ -1280,6 +1280,110 @@ int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const 
   return DPG_OK;
 }
 
+// Field recovery after the global solve (CondensedDofInterpreter::
+// interpretGlobalCoefficients, CondensedDofInterpreter.cpp:1229-1346): per cell,
+// K_ff u_f = l_f - K_ft t for the field dofs u_f given the cell's trace dofs t, with
+// the local K, l of the assembly (user numbering: fields first).  One CTA per cell:
+// K_ff is equilibrated (s_i = K_ii^-1/2) and Cholesky-factored in shared memory; the
+// local coefficients [u_f | t] are written out.  info: 0, or the first non-positive
+// pivot (1-based).
+namespace {
+__global__ void __launch_bounds__(256) recover_fields_kernel(int C, int M, int nf, const double* __restrict__ K,
+                                                             const double* __restrict__ l,
+                                                             const double* __restrict__ t_in, double* __restrict__ u,
+                                                             int32_t* __restrict__ info) {
+  extern __shared__ double rs[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int nt = M - nf;
+  double* A = rs;                 // nf x nf, row-major (lower triangle used)
+  double* sc = A + nf * nf;       // scaling
+  double* b = sc + nf;            // right-hand side, then the solution
+  __shared__ int fail;
+  for (int cell = blockIdx.x; cell < C; cell += gridDim.x) {
+    const double* Kc = K + (size_t)cell * M * M;
+    const double* lc = l + (size_t)cell * M;
+    const double* tc = t_in + (size_t)cell * nt;
+    if (tid == 0) fail = 0;
+    for (int i = tid; i < nf; i += blockDim.x) {
+      const double d = Kc[(size_t)i * M + i];
+      sc[i] = d > 0.0 ? rsqrt(d) : 1.0;
+    }
+    __syncthreads();
+    for (int e = tid; e < nf * nf; e += blockDim.x) {
+      const int i = e / nf, j = e - i * nf;
+      A[e] = sc[i] * Kc[(size_t)i * M + j] * sc[j];
+    }
+    // b = S (l_f - K_ft t): one warp per row
+    for (int i = warp; i < nf; i += nw) {
+      double acc = 0.0;
+      for (int j = lane; j < nt; j += 32) acc += Kc[(size_t)i * M + nf + j] * tc[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) b[i] = sc[i] * (lc[i] - acc);
+    }
+    __syncthreads();
+    // right-looking Cholesky, column by column
+    for (int k = 0; k < nf; k++) {
+      const double piv = A[k * nf + k];
+      if (!(piv > 0.0)) {
+        if (tid == 0 && fail == 0) fail = k + 1;
+      }
+      const double inv = rsqrt(piv);
+      __syncthreads();
+      for (int i = k + tid; i < nf; i += blockDim.x) A[i * nf + k] = (i == k) ? piv * inv : A[i * nf + k] * inv;
+      __syncthreads();
+      const int m = nf - 1 - k;
+      for (int e = tid; e < m * m; e += blockDim.x) {
+        const int i = k + 1 + e / m, j = k + 1 + e % m;
+        if (j <= i) A[i * nf + j] -= A[i * nf + k] * A[j * nf + k];
+      }
+      __syncthreads();
+    }
+    // L z = b, L^T y = z (warp 0; lanes split the dot products)
+    if (warp == 0) {
+      for (int i = 0; i < nf; i++) {
+        double acc = 0.0;
+        for (int j = lane; j < i; j += 32) acc += A[i * nf + j] * b[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) b[i] = (b[i] - acc) / A[i * nf + i];
+        __syncwarp();
+      }
+      for (int i = nf - 1; i >= 0; i--) {
+        double acc = 0.0;
+        for (int j = i + 1 + lane; j < nf; j += 32) acc += A[j * nf + i] * b[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) b[i] = (b[i] - acc) / A[i * nf + i];
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    double* uc = u + (size_t)cell * M;
+    for (int i = tid; i < M; i += blockDim.x) uc[i] = i < nf ? sc[i] * b[i] : tc[i - nf];
+    if (tid == 0 && info) info[cell] = fail;
+    __syncthreads();
+  }
+}
+}  // namespace
+
+int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const double* l, const double* t, double* u,
+                              int32_t* info, cudaStream_t stream) {
+  if (C <= 0) return DPG_OK;
+  const size_t bytes = ((size_t)nf * nf + 2 * (size_t)nf) * sizeof(double);
+  if (bytes > 200 * 1024) return dpg::fail(DPG_ERR_UNSUPPORTED, "too many field dofs for the recovery kernel");
+  static int configured = 0;
+  if (!configured) {
+    cudaFuncSetAttribute(recover_fields_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    configured = 1;
+  }
+  const int grid = std::min(C, (g_num_sms > 0 ? g_num_sms : 148) * 4);
+  recover_fields_kernel<<<grid, 256, bytes, stream>>>(C, M, nf, K, l, t, u, info);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
 // Bounded-wait probe: one thread waits, with the kernels' own wait routine, on an
 // mbarrier whose transaction never arrives (a flag nothing sets), and reports the
 // status the assembly kernels turn into info = 0x7fff0000.  Lets a test check that a

@@ -52,6 +52,7 @@ def load():
     L.dpg_factored_cholesky_solve.argtypes = [i, i, i] + [vp] * 6 + [vp]
     L.dpg_assemble_adjoint.argtypes = [vp, i] + [vp] * 7 + [vp]
     L.dpg_assemble_multi.argtypes = [i, vp, vp, i]
+    L.dpg_recover_fields.argtypes = [vp, i] + [vp] * 5 + [vp]
     L.dpg_graph_capture.argtypes = [i, vp, i, ct.POINTER(vp)]
     L.dpg_graph_launch.argtypes = [vp, vp]
     L.dpg_graph_destroy.argtypes = [vp]
@@ -155,6 +156,17 @@ class Plan:
                                            _ptr(Kbar.contiguous()), _ptr(None if lbar is None else lbar.contiguous()),
                                            _ptr(cbar), _ptr(info), _stream_ptr(stream)))
         return cbar, info
+
+    def recover_fields(self, K, l, trace_coeff, stream=None):
+        """dpg_recover_fields: local coefficients [u_f | t] (C, M) from K, l and the cells'
+        trace coefficients t (C, n_trace) after the global solve; device tensors."""
+        import torch
+        C = K.shape[0]
+        u = torch.empty((C, self.info["M"]), dtype=torch.float64, device=K.device)
+        info = torch.empty((C,), dtype=torch.int32, device=K.device)
+        _check(load().dpg_recover_fields(self.h, C, _ptr(K.contiguous()), _ptr(l.contiguous()),
+                                         _ptr(trace_coeff.contiguous()), _ptr(u), _ptr(info), _stream_ptr(stream)))
+        return u, info
 
     # -------------------------------------------------------------------- host
     def assemble_host(self, nodes, parity, coeff=None, out=None, flags=0):

@@ -40,6 +40,8 @@
  *                             TRHS::integrateAgainstStandardBasis (src/Problem/RHS.cpp:68-82)
  *   dpg_factored_cholesky_solve  TBF::factoredCholeskySolve (src/ScratchPad/BF.cpp:924-1018)
  *   dpg_assemble_adjoint      no counterpart in the reference (new capability)
+ *   dpg_recover_fields        CondensedDofInterpreter::interpretGlobalCoefficients
+ *                             (src/Solution/CondensedDofInterpreter.cpp:1229-1346)
  */
 #ifndef DPG_B200_H
 #define DPG_B200_H
@@ -218,6 +220,16 @@ int dpg_factored_cholesky_solve(int C, int N, int M, const double* G, const doub
 int dpg_assemble_adjoint(dpg_plan* plan, int C, const double* nodes, const int8_t* parity,
                          const double* coeff, const double* Kbar, const double* lbar,
                          double* coeff_bar, int32_t* info, void* stream);
+
+/* Field back-substitution after the global (trace) solve: replaces
+ * CondensedDofInterpreter::interpretGlobalCoefficients
+ * (src/Solution/CondensedDofInterpreter.cpp:1229-1346).  For each cell solves
+ * K_ff u_f = l_f - K_ft t with the cell's K (C,M,M) and l (C,M) from dpg_assemble
+ * (user numbering, fields first) and its trace coefficients t (C, n_trace), and
+ * writes the local coefficients [u_f | t] to local_coeff (C,M).  info[c] = first
+ * non-positive pivot of the equilibrated K_ff (1-based) or 0.  Device pointers. */
+int dpg_recover_fields(dpg_plan* plan, int C, const double* K, const double* l, const double* trace_coeff,
+                       double* local_coeff, int32_t* info, void* stream);
 
 /* Multi-bucket assembly (TSolution::populateStiffnessAndLoad's loop over
  * ElementType buckets, Solution.cpp:1131-1297): one persistent launch walks the
