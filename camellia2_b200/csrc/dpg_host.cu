@@ -1569,6 +1569,23 @@ static int multi_args(int n_buckets, const dpg_bucket_batch* buckets, int flags,
   return DPG_OK;
 }
 
+int dpg_energy_error(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                     const double* local_coeff, double* energy, int32_t* info, void* stream) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!nodes || !parity || !local_coeff || !energy || !info)
+    return fail(DPG_ERR_INVALID_ARGUMENT, "nodes, parity, local coefficients, energy and info are required");
+  if (p->hp.dev.nslots > 0 && !coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.nodes = nodes; L.parity = parity; L.coeff = coeff;
+  L.info = info;
+  L.xsol = local_coeff;
+  L.energy = energy;
+  return dpg_launch_energy(&p->hp.dev, &L, (cudaStream_t)stream);
+}
+
 int dpg_recover_fields(dpg_plan* p, int C, const double* K, const double* l, const double* trace_coeff,
                        double* local_coeff, int32_t* info, void* stream) {
   if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");

@@ -39,6 +39,9 @@ struct DpgLaunch {
   const double* lbar;
   double* coeff_bar;
   double* scratch2;
+  // dpg_energy_error: local trial coefficients in (C, M), energy error out (C)
+  const double* xsol;
+  double* energy;
 };
 
 int dpg_configure_kernels(const DpgPlanDev* plan);
@@ -49,6 +52,7 @@ int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d
 int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
+int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const double* l, const double* t, double* u,
                               int32_t* info, cudaStream_t stream);
 

@@ -1198,6 +1198,8 @@ __global__ void __launch_bounds__(NT, 1) dpg_multi_kernel(const DpgPlanDev* __re
   }
 }
 
+#include "dpg_energy.cuh"
+
 typedef void (*MultiFn)(const DpgPlanDev*, const DpgLaunch*, const int*, int);
 #define DPG_MULTI_INSTANCES(X) X(16, 6, 4) X(24, 12, 6)
 
@@ -1427,6 +1429,32 @@ int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_
   size_t bytes = (size_t)plan->sm_total * sizeof(double);
   k<<<grid, NT, bytes, stream>>>(*plan, L);
   cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(scratch, stream);
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
+int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
+  if (Lin->C <= 0) return DPG_OK;
+  KernelFn k = pick_energy_kernel(plan);
+  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no energy-error kernel instance for this bucket size");
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       optin > 0 ? optin : (int)(plan->sm_total * sizeof(double)));
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  DpgLaunch L = *Lin;
+  void* scratch = nullptr;
+  cudaError_t ea = cudaMallocAsync(&scratch, (size_t)grid * plan->scratch_per_cta * sizeof(double), stream);
+  if (ea != cudaSuccess) {
+    cudaGetLastError();
+    return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(ea));
+  }
+  L.scratch = (double*)scratch;
+  k<<<grid, NT, (size_t)plan->sm_total * sizeof(double), stream>>>(*plan, L);
+  e = cudaGetLastError();
   cudaFreeAsync(scratch, stream);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;

@@ -53,6 +53,7 @@ def load():
     L.dpg_assemble_adjoint.argtypes = [vp, i] + [vp] * 7 + [vp]
     L.dpg_assemble_multi.argtypes = [i, vp, vp, i]
     L.dpg_recover_fields.argtypes = [vp, i] + [vp] * 5 + [vp]
+    L.dpg_energy_error.argtypes = [vp, i] + [vp] * 6 + [vp]
     L.dpg_graph_capture.argtypes = [i, vp, i, ct.POINTER(vp)]
     L.dpg_graph_launch.argtypes = [vp, vp]
     L.dpg_graph_destroy.argtypes = [vp]
@@ -156,6 +157,17 @@ class Plan:
                                            _ptr(Kbar.contiguous()), _ptr(None if lbar is None else lbar.contiguous()),
                                            _ptr(cbar), _ptr(info), _stream_ptr(stream)))
         return cbar, info
+
+    def energy_error(self, nodes, parity, coeff, local_coeff, stream=None):
+        """dpg_energy_error: per-cell energy error sqrt(r^T G^-1 r), r = F - B x, of the
+        local trial coefficients x (C, M); device tensors."""
+        import torch
+        C = nodes.shape[0]
+        e = torch.empty((C,), dtype=torch.float64, device=nodes.device)
+        info = torch.empty((C,), dtype=torch.int32, device=nodes.device)
+        _check(load().dpg_energy_error(self.h, C, _ptr(nodes), _ptr(parity), _ptr(coeff), _ptr(local_coeff.contiguous()),
+                                       _ptr(e), _ptr(info), _stream_ptr(stream)))
+        return e, info
 
     def recover_fields(self, K, l, trace_coeff, stream=None):
         """dpg_recover_fields: local coefficients [u_f | t] (C, M) from K, l and the cells'

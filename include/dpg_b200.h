@@ -40,6 +40,8 @@
  *                             TRHS::integrateAgainstStandardBasis (src/Problem/RHS.cpp:68-82)
  *   dpg_factored_cholesky_solve  TBF::factoredCholeskySolve (src/ScratchPad/BF.cpp:924-1018)
  *   dpg_assemble_adjoint      no counterpart in the reference (new capability)
+ *   dpg_energy_error          TSolution::rankLocalEnergyError, computeErrorRepresentation
+ *                             (src/Solution/Solution.cpp:2653-2722)
  *   dpg_recover_fields        CondensedDofInterpreter::interpretGlobalCoefficients
  *                             (src/Solution/CondensedDofInterpreter.cpp:1229-1346)
  */
@@ -230,6 +232,14 @@ int dpg_assemble_adjoint(dpg_plan* plan, int C, const double* nodes, const int8_
  * non-positive pivot of the equilibrated K_ff (1-based) or 0.  Device pointers. */
 int dpg_recover_fields(dpg_plan* plan, int C, const double* K, const double* l, const double* trace_coeff,
                        double* local_coeff, int32_t* info, void* stream);
+
+/* Energy error of a trial solution per cell: replaces TSolution::rankLocalEnergyError
+ * with computeErrorRepresentation (src/Solution/Solution.cpp:2653-2722).  For the
+ * cells' local trial coefficients x (C,M; user numbering, fields first) writes
+ * energy[c] = sqrt(r^T G^-1 r), r = F - B x the residual on the test space.
+ * info as for dpg_assemble.  Device pointers. */
+int dpg_energy_error(dpg_plan* plan, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                     const double* local_coeff, double* energy, int32_t* info, void* stream);
 
 /* Multi-bucket assembly (TSolution::populateStiffnessAndLoad's loop over
  * ElementType buckets, Solution.cpp:1131-1297): one persistent launch walks the
