@@ -1,28 +1,30 @@
 // dpg_kernel.cu — fused FP64 per-cell DPG assembly for sm_100a.
 //
 // Persistent CTAs (16 warps, one per SM) walk the cells.  Per cell:
-//   1. B and F (TBF::stiffnessMatrix, BF.cpp:575-656; RHS.cpp:68-82): per
-//      quadrature segment (volume, each side) the per-point records — reference
-//      slots of the test bases plus each term's trial values — arrive by bulk
-//      (TMA) copy, double buffered.  The Piola maps, normals, parities and
-//      coefficients of every term collapse into one 4-vector per point (R), the
-//      coupling U = R * trial values is formed per active (test var, column tile)
-//      block, and warp J accumulates B[:, J] in registers with mma.m8n8k4.f64
-//      (DMMA).  The tiles wait in a per-CTA scratch slot (L2-resident).
-//   2. Gram matrix G (IP::computeInnerProductMatrix, IP.cpp:215-292): the same
-//      slot form; per point and test-var pair a 4x4 coupling D = T_a^T C T_b
-//      (C: graph-norm coefficients, T: Piola maps) is built once, h = D * slots
-//      per chunk, and every warp accumulates a run of lower 8x8 tiles of G.
+//   1. B and F (TBF::stiffnessMatrix, BF.cpp:575-656; RHS.cpp:68-82).  Volume: the
+//      per-point records (reference slots of the test bases plus each term's trial
+//      values) arrive by bulk (TMA) copy, double buffered; U = (weight x coefficient
+//      x Piola row) x trial value per active (test var, column tile) block, and each
+//      warp accumulates its 16x8 blocks with mma.m16n8k16.f64 over k-steps of 4
+//      points x 4 slots.  Boundary terms with a cell-independent side transform
+//      (HGRAD value; HDIV normal trace by the Piola identity) are separable: compact
+//      per-entry sums over the test rows nonzero on the side.  The tiles wait in a
+//      per-CTA scratch slot (L2-resident).
+//   2. Gram matrix G (IP::computeInnerProductMatrix, IP.cpp:215-292): the same slot
+//      form; per point and coupled test-var pair a 4x4 coupling D = T_a^T C T_b (C:
+//      graph-norm coefficients, T: Piola maps), h = D x slots by DMMA per chunk, and
+//      each warp accumulates its 16x8 blocks of the lower triangle (m16n8k16).
 //   3. Equilibrated Cholesky of G (BF.cpp:944-982: DPOEQU scaling, DPOTRF('L'),
-//      unscaling), blocked right-looking on tiles held in shared memory.
-//   4. W = L^-1 [B | F] in registers (BF.cpp:987-988, 1013-1014): each warp runs
-//      a blocked forward substitution on its own column tile; diagonal blocks use
-//      precomputed inverses so every step is a DMMA.
+//      unscaling), blocked right-looking with look-ahead on 8x8 tiles in shared memory.
+//   4. W = L^-1 [B | F] in registers (BF.cpp:987-988, 1013-1014): each warp runs a
+//      blocked forward substitution on its own column tile; diagonal blocks use
+//      precomputed inverses, row pairs update with mma.m16n8k8.f64.
 //   5. K_ext = W^T W (DSYRK, BF.cpp:993-1005) including l = W^T y (BF.cpp:1016).
 //   6. Static condensation (CondensedDofInterpreter.cpp:1138-1192): the first
 //      field-tile steps of a blocked Cholesky of K_ext leave the Schur complement
 //      [S s; s^T .] in the trailing block.
-// Numerical failures are reported per cell in info (DPOTRF INFO semantics).
+// Numerical failures are reported per cell in info (DPOTRF INFO semantics).  The
+// reverse mode, the energy error and the multi-bucket launch reuse these phases.
 #include "../../include/dpg_b200.h"
 #include "dpg_internal.h"
 #include "dpg_plan.h"
