@@ -1569,6 +1569,18 @@ static int multi_args(int n_buckets, const dpg_bucket_batch* buckets, int flags,
   return DPG_OK;
 }
 
+int dpg_scatter_global(int C, int t, const int64_t* map_ptr, const int64_t* map_gid, const double* map_w,
+                       int64_t n_global, const int64_t* row_ptr, const int64_t* col_idx, const double* S,
+                       const double* s, double* values, double* rhs, int* missing, void* stream) {
+  if (C < 0 || t < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative size");
+  if (C == 0 || t == 0) return DPG_OK;
+  if (!map_ptr || !map_gid || !row_ptr || !col_idx || !S || !values || !missing)
+    return fail(DPG_ERR_INVALID_ARGUMENT, "map, graph, S, values and the missing counter are required");
+  if (n_global <= 0) return fail(DPG_ERR_INVALID_ARGUMENT, "empty global system");
+  return dpg_launch_scatter_global(C, t, map_ptr, map_gid, map_w, n_global, row_ptr, col_idx, S, s, values, rhs,
+                                   missing, (cudaStream_t)stream);
+}
+
 int dpg_energy_error(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff,
                      const double* local_coeff, double* energy, int32_t* info, void* stream) {
   if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");

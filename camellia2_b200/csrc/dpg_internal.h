@@ -53,6 +53,9 @@ int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
+int dpg_launch_scatter_global(int C, int t, const int64_t* ptr, const int64_t* gid, const double* w,
+                              int64_t n_global, const int64_t* row_ptr, const int64_t* col, const double* S,
+                              const double* s, double* values, double* rhs, int* missing, cudaStream_t stream);
 int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const double* l, const double* t, double* u,
                               int32_t* info, cudaStream_t stream);
 

@@ -1388,6 +1388,69 @@ int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const doubl
   return DPG_OK;
 }
 
+// Global assembly of the condensed cell matrices (GDAMinimumRule::interpretLocalData,
+// GDAMinimumRule.cpp:714-800, through LocalDofMapper's C, then the insertion into the
+// global system, Solution.cpp:1263-1293): values += sum_c C_c^T S_c C_c and
+// rhs += sum_c C_c^T s_c on a CSR graph the caller owns.  Local dof a of cell c
+// stands for sum_k w_k x[gid_k], k in [ptr[c t + a], ptr[c t + a + 1]).  One thread
+// per (cell, a, b) entry; targets are found by binary search in the sorted CSR row
+// and summed with atomics, so the last bits depend on the order of arrival.
+namespace {
+__device__ __forceinline__ long long csr_find(const int64_t* __restrict__ row_ptr, const int64_t* __restrict__ col,
+                                              int64_t r, int64_t c) {
+  long long lo = row_ptr[r], hi = row_ptr[r + 1] - 1;
+  while (lo <= hi) {
+    const long long mid = (lo + hi) >> 1;
+    const int64_t v = col[mid];
+    if (v == c) return mid;
+    if (v < c) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+__global__ void scatter_global_kernel(int C, int t, const int64_t* __restrict__ ptr, const int64_t* __restrict__ gid,
+                                      const double* __restrict__ w, int64_t n, const int64_t* __restrict__ row_ptr,
+                                      const int64_t* __restrict__ col, const double* __restrict__ S,
+                                      const double* __restrict__ sv, double* __restrict__ values,
+                                      double* __restrict__ rhs, int* __restrict__ missing) {
+  const long long tt = (long long)t * t;
+  const long long total = (long long)C * tt;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / tt);
+    const int ab = (int)(e - (long long)c * tt);
+    const int a = ab / t, b = ab - a * t;
+    const double sab = S[e];
+    const long long ia = (long long)c * t + a, ib = (long long)c * t + b;
+    for (int64_t ka = ptr[ia]; ka < ptr[ia + 1]; ka++) {
+      const double wa = w ? w[ka] : 1.0;
+      for (int64_t kb = ptr[ib]; kb < ptr[ib + 1]; kb++) {
+        const int64_t r = gid[ka], cc = gid[kb];
+        const long long pos = (r >= 0 && r < n && cc >= 0 && cc < n) ? csr_find(row_ptr, col, r, cc) : -1;
+        if (pos < 0) { atomicAdd(missing, 1); continue; }
+        atomicAdd(values + pos, wa * (w ? w[kb] : 1.0) * sab);
+      }
+    }
+    if (b == 0 && sv && rhs)
+      for (int64_t ka = ptr[ia]; ka < ptr[ia + 1]; ka++)
+        if (gid[ka] >= 0 && gid[ka] < n) atomicAdd(rhs + gid[ka], (w ? w[ka] : 1.0) * sv[ia]);
+  }
+}
+}  // namespace
+
+int dpg_launch_scatter_global(int C, int t, const int64_t* ptr, const int64_t* gid, const double* w,
+                              int64_t n_global, const int64_t* row_ptr, const int64_t* col, const double* S,
+                              const double* s, double* values, double* rhs, int* missing, cudaStream_t stream) {
+  if (C <= 0 || t <= 0) return DPG_OK;
+  const long long total = (long long)C * t * t;
+  const int grid = (int)std::min<long long>((total + 255) / 256, (long long)(g_num_sms > 0 ? g_num_sms : 148) * 16);
+  scatter_global_kernel<<<grid, 256, 0, stream>>>(C, t, ptr, gid, w, n_global, row_ptr, col, S, s, values, rhs,
+                                                  missing);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
 // Bounded-wait probe: one thread waits, with the kernels' own wait routine, on an
 // mbarrier whose transaction never arrives (a flag nothing sets), and reports the
 // status the assembly kernels turn into info = 0x7fff0000.  Lets a test check that a

@@ -54,6 +54,7 @@ def load():
     L.dpg_assemble_multi.argtypes = [i, vp, vp, i]
     L.dpg_recover_fields.argtypes = [vp, i] + [vp] * 5 + [vp]
     L.dpg_energy_error.argtypes = [vp, i] + [vp] * 6 + [vp]
+    L.dpg_scatter_global.argtypes = [i, i] + [vp] * 3 + [ct.c_int64] + [vp] * 8
     L.dpg_graph_capture.argtypes = [i, vp, i, ct.POINTER(vp)]
     L.dpg_graph_launch.argtypes = [vp, vp]
     L.dpg_graph_destroy.argtypes = [vp]
@@ -258,3 +259,16 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+def scatter_global(S, s, map_ptr, map_gid, map_w, n_global, row_ptr, col_idx, values, rhs=None, stream=None):
+    """dpg_scatter_global: values += sum_c C_c^T S_c C_c, rhs += sum_c C_c^T s_c on the
+    CSR graph (row_ptr, col_idx); returns the number of skipped entries.  Device tensors
+    (int64 maps and graph, float64 data)."""
+    import torch
+    C, t = S.shape[0], S.shape[1]
+    missing = torch.zeros((1,), dtype=torch.int32, device=S.device)
+    _check(load().dpg_scatter_global(C, t, _ptr(map_ptr), _ptr(map_gid), _ptr(map_w), int(n_global), _ptr(row_ptr),
+                                     _ptr(col_idx), _ptr(S.contiguous()), _ptr(None if s is None else s.contiguous()),
+                                     _ptr(values), _ptr(rhs), _ptr(missing), _stream_ptr(stream)))
+    return missing

@@ -40,6 +40,8 @@
  *                             TRHS::integrateAgainstStandardBasis (src/Problem/RHS.cpp:68-82)
  *   dpg_factored_cholesky_solve  TBF::factoredCholeskySolve (src/ScratchPad/BF.cpp:924-1018)
  *   dpg_assemble_adjoint      no counterpart in the reference (new capability)
+ *   dpg_scatter_global        GDAMinimumRule::interpretLocalData + global insertion
+ *                             (src/Mesh/GDAMinimumRule.cpp:714-800, src/Solution/Solution.cpp:1263-1293)
  *   dpg_energy_error          TSolution::rankLocalEnergyError, computeErrorRepresentation
  *                             (src/Solution/Solution.cpp:2653-2722)
  *   dpg_recover_fields        CondensedDofInterpreter::interpretGlobalCoefficients
@@ -240,6 +242,21 @@ int dpg_recover_fields(dpg_plan* plan, int C, const double* K, const double* l, 
  * info as for dpg_assemble.  Device pointers. */
 int dpg_energy_error(dpg_plan* plan, int C, const double* nodes, const int8_t* parity, const double* coeff,
                      const double* local_coeff, double* energy, int32_t* info, void* stream);
+
+/* Global assembly of condensed cell systems: replaces the GDA interpretation
+ * GDAMinimumRule::interpretLocalData (src/Mesh/GDAMinimumRule.cpp:714-800, C^T S C
+ * through the LocalDofMapper) and the insertion into the global matrix
+ * (src/Solution/Solution.cpp:1263-1293).  Local dof a of cell c stands for
+ * sum_k map_w[k] x[map_gid[k]], k in [map_ptr[c t + a], map_ptr[c t + a + 1])
+ * (map_w NULL: all weights 1).  Adds sum_c C_c^T S_c C_c into the values of the
+ * caller's CSR graph (n_global rows; row_ptr, col_idx sorted within rows) and
+ * sum_c C_c^T s_c into rhs (may be NULL); entries absent from the graph or with a
+ * global index outside [0, n_global) are counted in *missing (device int) and
+ * skipped.  S (C,t,t), s (C,t) as from dpg_assemble.  Device pointers;
+ * summation order (atomics) varies between runs in the last bits. */
+int dpg_scatter_global(int C, int t, const int64_t* map_ptr, const int64_t* map_gid, const double* map_w,
+                       int64_t n_global, const int64_t* row_ptr, const int64_t* col_idx, const double* S,
+                       const double* s, double* values, double* rhs, int* missing, void* stream);
 
 /* Multi-bucket assembly (TSolution::populateStiffnessAndLoad's loop over
  * ElementType buckets, Solution.cpp:1131-1297): one persistent launch walks the

@@ -1,0 +1,92 @@
+"""Global assembly of the condensed cell systems (dpg_scatter_global; the GDA
+interpretation C^T S C of GDAMinimumRule::interpretLocalData, GDAMinimumRule.cpp:
+714-800, and the insertion of Solution.cpp:1263-1293) on a caller-owned CSR graph.
+
+The cells' S, s come from the GPU assembly of a 2D Poisson mesh; each local trace dof
+maps to one or two global dofs with weights (as hanging-node constraints do).  The
+CSR values and the right-hand side must equal a dense accumulation of C^T S C and
+C^T s on the host; entries outside the graph are counted, not written."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from camellia2_b200 import lib as dlib  # noqa: E402
+from tests.helpers import coeffs_for, poisson2d  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(seed=0):
+    form, bucket, nodes, par = poisson2d(2, 2, 3, 3, 0.2)
+    plan = dlib.Plan(bucket)
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, plan.info, C)
+    out = plan.assemble(*(torch.as_tensor(x).cuda() for x in (nodes, par, co)))
+    torch.cuda.synchronize()
+    S, s = out["S"].cpu().numpy(), out["s"].cpu().numpy()
+    t = S.shape[1]
+    rng = np.random.default_rng(seed)
+    n = 40
+    ptr, gid, w = [0], [], []
+    for c in range(C):
+        for a in range(t):
+            for _ in range(rng.integers(1, 3)):
+                gid.append(int(rng.integers(0, n)))
+                w.append(float(rng.uniform(0.25, 1.0)))
+            ptr.append(len(gid))
+    return S, s, np.array(ptr), np.array(gid), np.array(w), n
+
+
+def _dense(S, s, ptr, gid, w, n):
+    C, t = S.shape[0], S.shape[1]
+    A, b = np.zeros((n, n)), np.zeros(n)
+    for c in range(C):
+        Cm = np.zeros((t, n))
+        for a in range(t):
+            for k in range(ptr[c * t + a], ptr[c * t + a + 1]):
+                Cm[a, gid[k]] += w[k]
+        A += Cm.T @ S[c] @ Cm
+        b += Cm.T @ s[c]
+    return A, b
+
+
+def _graph(A, drop=None):
+    rows, cols = np.nonzero(np.ones_like(A, dtype=bool) if drop is None else ~drop)
+    row_ptr = np.zeros(A.shape[0] + 1, dtype=np.int64)
+    np.add.at(row_ptr, rows + 1, 1)
+    return np.cumsum(row_ptr), cols.astype(np.int64)
+
+
+def test_scatter_matches_dense_accumulation():
+    S, s, ptr, gid, w, n = _setup()
+    A, b = _dense(S, s, ptr, gid, w, n)
+    row_ptr, col = _graph(A)
+    dev = lambda x: torch.as_tensor(x).cuda()  # noqa: E731
+    vals = torch.zeros(col.shape[0], dtype=torch.float64, device="cuda")
+    rhs = torch.zeros(n, dtype=torch.float64, device="cuda")
+    missing = dlib.scatter_global(dev(S), dev(s), dev(ptr), dev(gid), dev(w), n, dev(row_ptr), dev(col), vals, rhs)
+    torch.cuda.synchronize()
+    assert int(missing.item()) == 0
+    Ag = np.zeros((n, n))
+    v = vals.cpu().numpy()
+    for r in range(n):
+        Ag[r, col[row_ptr[r]:row_ptr[r + 1]]] = v[row_ptr[r]:row_ptr[r + 1]]
+    assert np.linalg.norm(Ag - A) <= 1e-12 * np.linalg.norm(A)
+    assert np.linalg.norm(rhs.cpu().numpy() - b) <= 1e-12 * np.linalg.norm(b)
+
+
+def test_entries_outside_the_graph_are_counted():
+    S, s, ptr, gid, w, n = _setup(1)
+    A, b = _dense(S, s, ptr, gid, w, n)
+    drop = np.zeros((n, n), dtype=bool)
+    drop[0, :] = True  # row 0 absent from the graph
+    row_ptr, col = _graph(A, drop)
+    gid = gid.copy()
+    gid[0] = n + 5  # an index outside the system
+    dev = lambda x: torch.as_tensor(x).cuda()  # noqa: E731
+    vals = torch.zeros(col.shape[0], dtype=torch.float64, device="cuda")
+    missing = dlib.scatter_global(dev(S), dev(s), dev(ptr), dev(gid), dev(w), n, dev(row_ptr), dev(col), vals)
+    torch.cuda.synchronize()
+    assert int(missing.item()) > 0
+    assert np.isfinite(vals.cpu().numpy()).all()
