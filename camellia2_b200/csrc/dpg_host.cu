@@ -1598,6 +1598,22 @@ int dpg_energy_error(dpg_plan* p, int C, const double* nodes, const int8_t* pari
   return dpg_launch_energy(&p->hp.dev, &L, (cudaStream_t)stream);
 }
 
+int dpg_assemble_dls(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff, double* W,
+                     double* y, int32_t* info, void* stream) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (C < 0) return fail(DPG_ERR_INVALID_ARGUMENT, "negative cell count");
+  if (C == 0) return DPG_OK;
+  if (!nodes || !parity || !W || !y || !info) return fail(DPG_ERR_INVALID_ARGUMENT, "nodes, parity, W, y and info are required");
+  if (p->hp.dev.nslots > 0 && !coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.nodes = nodes; L.parity = parity; L.coeff = coeff;
+  L.info = info;
+  L.B = W;
+  L.F = y;
+  return dpg_launch_energy(&p->hp.dev, &L, (cudaStream_t)stream);  // no trial solution: the DLS kernel
+}
+
 int dpg_recover_fields(dpg_plan* p, int C, const double* K, const double* l, const double* trace_coeff,
                        double* local_coeff, int32_t* info, void* stream) {
   if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");

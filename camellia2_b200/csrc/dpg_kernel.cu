@@ -1501,8 +1501,8 @@ int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_
 
 int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
   if (Lin->C <= 0) return DPG_OK;
-  KernelFn k = pick_energy_kernel(plan);
-  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no energy-error kernel instance for this bucket size");
+  KernelFn k = Lin->xsol ? pick_energy_kernel(plan) : pick_dls_kernel(plan);
+  if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);

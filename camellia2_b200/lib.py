@@ -54,6 +54,7 @@ def load():
     L.dpg_assemble_multi.argtypes = [i, vp, vp, i]
     L.dpg_recover_fields.argtypes = [vp, i] + [vp] * 5 + [vp]
     L.dpg_energy_error.argtypes = [vp, i] + [vp] * 6 + [vp]
+    L.dpg_assemble_dls.argtypes = [vp, i] + [vp] * 6 + [vp]
     L.dpg_scatter_global.argtypes = [i, i] + [vp] * 3 + [ct.c_int64] + [vp] * 8
     L.dpg_graph_capture.argtypes = [i, vp, i, ct.POINTER(vp)]
     L.dpg_graph_launch.argtypes = [vp, vp]
@@ -158,6 +159,18 @@ class Plan:
                                            _ptr(Kbar.contiguous()), _ptr(None if lbar is None else lbar.contiguous()),
                                            _ptr(cbar), _ptr(info), _stream_ptr(stream)))
         return cbar, info
+
+    def dls(self, nodes, parity, coeff=None, stream=None):
+        """dpg_assemble_dls: W = L^-1 B (C, M, N) and y = L^-1 F (C, N), G = L L^T."""
+        import torch
+        C = nodes.shape[0]
+        i = self.info
+        W = torch.empty((C, i["M"], i["N"]), dtype=torch.float64, device=nodes.device)
+        y = torch.empty((C, i["N"]), dtype=torch.float64, device=nodes.device)
+        info = torch.empty((C,), dtype=torch.int32, device=nodes.device)
+        _check(load().dpg_assemble_dls(self.h, C, _ptr(nodes), _ptr(parity), _ptr(coeff), _ptr(W), _ptr(y), _ptr(info),
+                                       _stream_ptr(stream)))
+        return W, y, info
 
     def energy_error(self, nodes, parity, coeff, local_coeff, stream=None):
         """dpg_energy_error: per-cell energy error sqrt(r^T G^-1 r), r = F - B x, of the

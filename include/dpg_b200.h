@@ -40,6 +40,7 @@
  *                             TRHS::integrateAgainstStandardBasis (src/Problem/RHS.cpp:68-82)
  *   dpg_factored_cholesky_solve  TBF::factoredCholeskySolve (src/ScratchPad/BF.cpp:924-1018)
  *   dpg_assemble_adjoint      no counterpart in the reference (new capability)
+ *   dpg_assemble_dls          TBF::localStiffnessMatrixAndRHS_DLS (src/ScratchPad/BF.cpp:1169-1306)
  *   dpg_scatter_global        GDAMinimumRule::interpretLocalData + global insertion
  *                             (src/Mesh/GDAMinimumRule.cpp:714-800, src/Solution/Solution.cpp:1263-1293)
  *   dpg_energy_error          TSolution::rankLocalEnergyError, computeErrorRepresentation
@@ -234,6 +235,13 @@ int dpg_assemble_adjoint(dpg_plan* plan, int C, const double* nodes, const int8_
  * non-positive pivot of the equilibrated K_ff (1-based) or 0.  Device pointers. */
 int dpg_recover_fields(dpg_plan* plan, int C, const double* K, const double* l, const double* trace_coeff,
                        double* local_coeff, int32_t* info, void* stream);
+
+/* DLS local matrices: replaces TBF::localStiffnessMatrixAndRHS_DLS
+ * (src/ScratchPad/BF.cpp:1169-1306), whose factored solve leaves W = L^-1 B in the
+ * "stiffnessEnriched" array and y = L^-1 F in the enriched load (G = L L^T).
+ * W (C,M,N) trial x test and y (C,N), user numbering.  Device pointers. */
+int dpg_assemble_dls(dpg_plan* plan, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                     double* W, double* y, int32_t* info, void* stream);
 
 /* Energy error of a trial solution per cell: replaces TSolution::rankLocalEnergyError
  * with computeErrorRepresentation (src/Solution/Solution.cpp:2653-2722).  For the
