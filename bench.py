@@ -32,13 +32,17 @@ import numpy as np  # noqa: E402
 METRIC = "condensed DPG cells/s on 1 B200: mixed vs FP64 form at ≤1e-10 rel err"
 # Algorithmic work per c5 cell (reference's operation count: full contractions,
 # N^3/3 Cholesky, full TRSM, lower SYRK, condensation): 26.40 MFLOP.
-def algorithmic_flops_per_cell(N, M, nf, nt, QG, QB, QS, nsides, d):
+def flops_parts(N, M, nf, nt, QG, QB, QS, nsides, d):
     nv, ntau = 64, 108  # c5 test var sizes (v: HGRAD C3 hex, tau: HDIV I3 hex)
     FG = 2 * ntau * ntau * QG * 1 + 2 * N * N * QG * d + 2 * nv * nv * QG + 2 * ntau * ntau * QG * d
     FB = 2 * (8 * ntau + 24 * ntau * d + 24 * nv * d) * QB + nsides * 2 * (9 * ntau + 4 * nv) * QS
     Fsolve = N ** 3 / 3 + N * N * M + N * M * (M + 1) + N * N + 2 * N * M
     Fcond = 2 * nf ** 3 / 3 + 2 * nf * nf * nt + 2 * nt * nt * nf + 2 * nf * nf + 2 * nt * nf
-    return FG + FB + Fsolve + Fcond
+    return FG, FB, Fsolve, Fcond
+
+
+def algorithmic_flops_per_cell(*a):
+    return sum(flops_parts(*a))
 
 
 def parse():
@@ -129,6 +133,88 @@ def other_configs(torch):
         total += C
     ms = timeit(lambda: lib.assemble_multi(items))
     res["c3_stokes_quads_p1_2_tris_p1_3_multi"] = {"cells": total, "ms": ms, "cells_per_s": total / ms * 1e3}
+    return res
+
+
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this GPU model (MEASURED_PEAKS.json beside this file)."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def next_rows(torch, plan, info, n, d_nodes, d_par, d_co, out, peak_tflops, hbm_gbs):
+    """The per-cell kernels that follow the assembly (field recovery, energy error, DLS
+    local matrices, global scatter of S, s) timed on the same 48^3 workload, inputs
+    resident (CUDA events, 3 launches after one warm-up), each with its roofline."""
+    from camellia2_b200 import lib, mesh
+
+    def timeit(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    C, M, N, nf, nt = d_nodes.shape[0], info["M"], info["N"], info["n_field"], info["n_trace"]
+    FG, FB, _, _ = flops_parts(N, M, nf, nt, info["Q_G"], info["Q_B"], info["Q_side"], info["n_sides"],
+                               info["space_dim"])
+    res = {}
+    g = torch.Generator(device=d_nodes.device).manual_seed(7)
+    tr = torch.rand((C, nt), dtype=torch.float64, device=d_nodes.device, generator=g) * 2 - 1
+    u = [None]
+
+    def rec():
+        u[0], _ = plan.recover_fields(out["K"], out["l"], tr)
+    ms = timeit(rec)
+    by = 8 * (nf * M + nf + nt + M)  # K rows of the fields (K_ff | K_ft), l_f, t in; u out
+    res["recover_fields"] = {"ms": ms, "cells_per_s": C / ms * 1e3, "bound": "hbm", "bytes_per_cell": by,
+                             "achieved_gbs": by * C / ms * 1e-6, "frac_of_measured_hbm": by * C / ms * 1e-6 / hbm_gbs}
+    fl = FG + FB + N ** 3 / 3 + N * N + 2 * N * M + 2 * N
+    ms = timeit(lambda: plan.energy_error(d_nodes, d_par, d_co, u[0]))
+    res["energy_error"] = {"ms": ms, "cells_per_s": C / ms * 1e3, "bound": "tensor", "flops_per_cell": fl,
+                           "achieved_tflops": fl * C / ms * 1e-9, "frac_of_measured_fp64": fl * C / ms * 1e-9 / peak_tflops}
+    del u[0]
+    fl = FG + FB + N ** 3 / 3 + N * N * M + N * N
+    ms = timeit(lambda: plan.dls(d_nodes, d_par, d_co))
+    res["dls"] = {"ms": ms, "cells_per_s": C / ms * 1e3, "bound": "tensor", "flops_per_cell": fl,
+                  "achieved_tflops": fl * C / ms * 1e-9, "frac_of_measured_fp64": fl * C / ms * 1e-9 / peak_tflops,
+                  "out_bytes_per_cell": 8 * (M * N + N)}
+    torch.cuda.empty_cache()
+    # global scatter with the conforming-shaped trace map of the hex grid
+    gid_np, ng = mesh.hex_trace_map(n, n, n, 2)
+    gid = torch.as_tensor(gid_np, device=d_nodes.device)
+    keys = (gid[:, :, None] * ng + gid[:, None, :]).reshape(-1)
+    keys = torch.unique(keys)
+    rows, cols = keys // ng, keys % ng
+    del keys
+    row_ptr = torch.zeros(ng + 1, dtype=torch.int64, device=d_nodes.device)
+    row_ptr[1:] = torch.cumsum(torch.bincount(rows, minlength=ng), 0)
+    del rows
+    nnz = cols.shape[0]
+    ptr = torch.arange(C * nt + 1, dtype=torch.int64, device=d_nodes.device)
+    gflat = gid.reshape(-1).contiguous()
+    vals = torch.empty(nnz, dtype=torch.float64, device=d_nodes.device)
+    rhs = torch.empty(ng, dtype=torch.float64, device=d_nodes.device)
+    miss = [None]
+
+    def scat():
+        vals.zero_()
+        rhs.zero_()
+        miss[0] = lib.scatter_global(out["S"], out["s"], ptr, gflat, None, ng, row_ptr, cols, vals, rhs)
+    ms = timeit(scat)
+    by = 8 * C * (nt * nt + nt) + 16 * C * nt + 16 * nnz + 8 * (ng + 1) + 8 * ng
+    res["scatter_global"] = {"ms": ms, "cells_per_s": C / ms * 1e3, "bound": "hbm", "n_global": ng, "nnz": nnz,
+                             "bytes": by, "achieved_gbs": by / ms * 1e-6, "frac_of_measured_hbm": by / ms * 1e-6 / hbm_gbs,
+                             "missing": int(miss[0].item()),
+                             "map": "hex trace points identified by lattice position (50 global dofs per cell)"}
+    del vals, cols, row_ptr
+    torch.cuda.empty_cache()
     return res
 
 
@@ -322,7 +408,7 @@ def main():
     bad = int((out["info"] != 0).sum().item())
 
     # ---- end to end through the host C-ABI call (pinned host buffers) -----------
-    e2e = None
+    e2e = e2e_cond = None
     if not args.no_e2e:
         h_nodes = torch.as_tensor(nodes).pin_memory()
         h_par = torch.as_tensor(par).pin_memory()
@@ -350,6 +436,22 @@ def main():
         e2e = {"value": world * C / (ems * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": ems,
                "path": "dpg_assemble_host (C ABI), pinned host buffers, 2-stream chunked copies"}
+        # The same call with DPG_FLAG_NO_K: only the condensed S, s come back (the reference's
+        # CondensedDofInterpreter recomputes K per cell when it holds none, CondensedDofInterpreter.cpp:106).
+        hc = {"S": hout["S"], "s": hout["s"], "info": hout["info"], "K": None, "l": None}
+        plan.assemble_host(h_nodes, h_par, h_co, out=hc, flags=1)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0.record(stream)
+        for _ in range(e_steps):
+            plan.assemble_host(h_nodes, h_par, h_co, out=hc, flags=1)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        cms = max_over_ranks(f0.elapsed_time(f1) / e_steps, dev)
+        e2e_cond = {"value": world * C / (cms * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": sum(x.numel() * x.element_size() for x in (hout["S"], hout["s"], hout["info"])),
+                    "ms_per_step": cms, "path": "dpg_assemble_host with DPG_FLAG_NO_K (S, s and info only)"}
 
     if rank == 0:
         peak = fp64_peak_tflops(torch)
@@ -383,11 +485,14 @@ def main():
                          "flops_per_cell": fl, "peak_source": "measured live: torch float64 GEMM 8192^3 (DMMA d884), FP64 tensor pipe"},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "e2e_condensed": e2e_cond,
             "gpu_launches": args.steps,
             "clocks": clocks,
             "parity_vs_oracle_max_rel": parity,
             "info_nonzero_cells": bad,
             "other_configs": None if args.no_extra else other_configs(torch),
+            "next_rows": None if args.no_extra else next_rows(torch, plan, info, n, d_nodes, d_par, d_co, out, peak,
+                                                              measured_hbm_gbs()),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -9,7 +9,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", f) for f in ("dpg_host.cu", "dpg_kernel.cu")]
+SRC = [os.path.join(HERE, "csrc", f) for f in ("dpg_host.cu", "dpg_kernel.cu", "dpg_maps.cu")]
 OUT = os.path.join(HERE, "libdpg_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

@@ -56,6 +56,8 @@ def load():
     L.dpg_energy_error.argtypes = [vp, i] + [vp] * 6 + [vp]
     L.dpg_assemble_dls.argtypes = [vp, i] + [vp] * 6 + [vp]
     L.dpg_scatter_global.argtypes = [i, i] + [vp] * 3 + [ct.c_int64] + [vp] * 8
+    L.dpg_compose_map.argtypes = [i, i] + [vp] * 3 + [ct.c_int64] + [vp] * 6 + [ct.c_int64, ct.POINTER(ct.c_int64),
+                                                                               vp, vp]
     L.dpg_graph_capture.argtypes = [i, vp, i, ct.POINTER(vp)]
     L.dpg_graph_launch.argtypes = [vp, vp]
     L.dpg_graph_destroy.argtypes = [vp]
@@ -285,3 +287,22 @@ def scatter_global(S, s, map_ptr, map_gid, map_w, n_global, row_ptr, col_idx, va
                                      _ptr(col_idx), _ptr(S.contiguous()), _ptr(None if s is None else s.contiguous()),
                                      _ptr(values), _ptr(rhs), _ptr(missing), _stream_ptr(stream)))
     return missing
+
+
+def compose_map(C, t, map_ptr, map_gid, map_w, n_fine, p_row_ptr, p_col, p_val, stream=None):
+    """dpg_compose_map: the per-cell local-to-coarse maps C_c P (size query, then fill).
+    Returns (ptr, gid, w, missing) as device tensors; scatter_global with them and the
+    cells' S, s assembles the Galerkin coarse operator P^T A P and load P^T b."""
+    import torch
+    dev = map_ptr.device
+    L, sp = load(), _stream_ptr(stream)
+    out_ptr = torch.empty((C * t + 1,), dtype=torch.int64, device=dev)
+    missing = torch.zeros((1,), dtype=torch.int32, device=dev)
+    n = ct.c_int64(0)
+    args = (_ptr(map_ptr), _ptr(map_gid), _ptr(map_w), int(n_fine), _ptr(p_row_ptr), _ptr(p_col), _ptr(p_val))
+    _check(L.dpg_compose_map(C, t, *args, _ptr(out_ptr), None, None, 0, ct.byref(n), _ptr(missing), sp))
+    gid = torch.empty((max(n.value, 1),), dtype=torch.int64, device=dev)
+    w = torch.empty((max(n.value, 1),), dtype=torch.float64, device=dev)
+    missing.zero_()
+    _check(L.dpg_compose_map(C, t, *args, _ptr(out_ptr), _ptr(gid), _ptr(w), n.value, ct.byref(n), _ptr(missing), sp))
+    return out_ptr, gid[:n.value], w[:n.value], missing

@@ -98,6 +98,41 @@ def hex_grid(nx, ny, nz, jitter=0.0, seed=1, extent=(1.0, 1.0, 1.0)):
     return np.ascontiguousarray(nodes), par
 
 
+def hex_trace_map(nx, ny, nz, k=2):
+    """Conforming-shaped local-to-global map of the hex Poisson UW traces on hex_grid's
+    cells: the H1 trace (k+1)^2 points per face and the L2 flux trace k^2 dofs per face,
+    numbered face by face (faces x-, x+, y-, y+, z-, z+; points i + (k+1) j on the face's two
+    tangent axes in increasing order).  Points are identified by their lattice position, so
+    a trace point on a shared vertex, edge or face gets one global id for all the cells
+    and faces touching it, as the GDA map of a conforming mesh does.  Returns gid (C, t)
+    int64 with dense ids and the number of global dofs."""
+    P = k * max(nx, ny, nz) + 1
+    dims = (nx, ny, nz)
+    kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    idx = np.stack([ii.reshape(-1), jj.reshape(-1), kk.reshape(-1)], axis=1)  # (C, 3), cell id = i + nx (j + ny k)
+    C = idx.shape[0]
+    nh, nq = (k + 1) ** 2, k * k
+    h1 = np.empty((C, 6, nh), np.int64)
+    fl = np.empty((C, 6, nq), np.int64)
+    a_i, b_i = np.meshgrid(np.arange(k + 1), np.arange(k + 1), indexing="xy")  # point i + (k+1) j
+    a_i, b_i = a_i.reshape(-1), b_i.reshape(-1)
+    nfaces = [(dims[a] + 1) * dims[(a + 1) % 3] * dims[(a + 2) % 3] for a in range(3)]
+    face_base = np.cumsum([0] + nfaces)
+    for f in range(6):
+        a, side = f // 2, f % 2
+        b, c = [x for x in range(3) if x != a]
+        pos = np.empty((C, nh, 3), np.int64)
+        pos[:, :, a] = (k * (idx[:, a] + side))[:, None]
+        pos[:, :, b] = k * idx[:, b][:, None] + a_i[None, :]
+        pos[:, :, c] = k * idx[:, c][:, None] + b_i[None, :]
+        h1[:, f] = pos[:, :, 0] + P * (pos[:, :, 1] + P * pos[:, :, 2])
+        fid = face_base[a] + ((idx[:, a] + side) * dims[b] + idx[:, b]) * dims[c] + idx[:, c]
+        fl[:, f] = P ** 3 + fid[:, None] * nq + np.arange(nq)[None, :]
+    raw = np.concatenate([h1.reshape(C, -1), fl.reshape(C, -1)], axis=1)
+    uniq, inv = np.unique(raw, return_inverse=True)
+    return inv.reshape(C, -1).astype(np.int64), int(uniq.shape[0])
+
+
 def uniform_coeff(C, n_slots, n_points, low=-1.0, high=1.0, seed=1):
     rng = np.random.default_rng(seed)
     return rng.uniform(low, high, size=(C, n_slots, n_points))

@@ -43,6 +43,9 @@
  *   dpg_assemble_dls          TBF::localStiffnessMatrixAndRHS_DLS (src/ScratchPad/BF.cpp:1169-1306)
  *   dpg_scatter_global        GDAMinimumRule::interpretLocalData + global insertion
  *                             (src/Mesh/GDAMinimumRule.cpp:714-800, src/Solution/Solution.cpp:1263-1293)
+ *   dpg_compose_map           GMGOperator::computeCoarseStiffnessMatrix's P^T A P, as
+ *                             per-cell maps C_c P for dpg_scatter_global
+ *                             (src/Solution/GMGOperator.cpp:173-366,420-773)
  *   dpg_energy_error          TSolution::rankLocalEnergyError, computeErrorRepresentation
  *                             (src/Solution/Solution.cpp:2653-2722)
  *   dpg_recover_fields        CondensedDofInterpreter::interpretGlobalCoefficients
@@ -265,6 +268,27 @@ int dpg_energy_error(dpg_plan* plan, int C, const double* nodes, const int8_t* p
 int dpg_scatter_global(int C, int t, const int64_t* map_ptr, const int64_t* map_gid, const double* map_w,
                        int64_t n_global, const int64_t* row_ptr, const int64_t* col_idx, const double* S,
                        const double* s, double* values, double* rhs, int* missing, void* stream);
+
+/* Local-to-coarse maps for a Galerkin multigrid coarse operator.  Replaces the
+ * sparse triple product P^T A P of GMGOperator::computeCoarseStiffnessMatrix
+ * (src/Solution/GMGOperator.cpp:173-366), A the assembled fine matrix and P the
+ * prolongation from the fine cells' LocalDofMappers (GMGOperator.cpp:420-773,
+ * 959-1551): since P^T A P = sum_c (C_c P)^T S_c (C_c P), this call composes each
+ * cell's local-to-fine map (map_ptr, map_gid, map_w as for dpg_scatter_global,
+ * C*t rows, n_fine global dofs) with P (CSR: n_fine rows P_row_ptr, coarse column
+ * ids P_col, values P_val), and dpg_scatter_global with the composed map and the
+ * cells' S, s assembles the coarse operator and load.  Outputs: out_ptr (C*t+1
+ * row offsets), and, when out_gid is not NULL, out_gid / out_w (coarse ids and
+ * weights map_w[k] * P_val[j], in the order of k then j; repeated coarse ids are
+ * kept).  *out_count (host) receives the number of composed entries; a call with
+ * out_gid NULL is the size query.  Fails with DPG_ERR_INVALID_ARGUMENT when that
+ * number exceeds capacity.  Map entries with a fine id outside [0, n_fine) are
+ * skipped and added to *missing (device int, may be NULL) on every call.  Device
+ * pointers except out_count; the call waits for the stream once (the count). */
+int dpg_compose_map(int C, int t, const int64_t* map_ptr, const int64_t* map_gid, const double* map_w,
+                    int64_t n_fine, const int64_t* P_row_ptr, const int64_t* P_col, const double* P_val,
+                    int64_t* out_ptr, int64_t* out_gid, double* out_w, int64_t capacity,
+                    int64_t* out_count, int* missing, void* stream);
 
 /* Multi-bucket assembly (TSolution::populateStiffnessAndLoad's loop over
  * ElementType buckets, Solution.cpp:1131-1297): one persistent launch walks the

@@ -108,6 +108,19 @@ def test_host_api_matches_device_api(cases):
         assert np.array_equal(h[k], d[k].cpu().numpy()), k
 
 
+@pytest.mark.parametrize("flags,kept", [(1, ("S", "s", "info")), (2, ("K", "l", "info"))])
+def test_host_api_output_flags(cases, flags, kept):
+    """DPG_FLAG_NO_K (1) returns S, s alone, DPG_FLAG_NO_CONDENSE (2) K, l alone; what is
+    returned equals the full call bit for bit."""
+    bucket, nodes, par, co, ref, info = cases["poisson3d_k2_dk1"]
+    plan = dlib.Plan(bucket)
+    full = plan.assemble_host(nodes, par, co)
+    part = {k: (np.empty_like(full[k]) if k in kept else None) for k in ("K", "l", "S", "s", "info")}
+    plan.assemble_host(nodes, par, co, out=part, flags=flags)
+    for k in kept:
+        assert np.array_equal(part[k], full[k]), k
+
+
 def test_empty_batch_is_ok(cases):
     bucket, nodes, par, co, ref, info = cases["poisson2d_k2_dk2"]
     plan = dlib.Plan(bucket)
