@@ -340,7 +340,7 @@ __device__ __forceinline__ void phase_adj_pull(const DpgPlanDev& P, const DpgLau
   __syncthreads();
 }
 
-template <int NBTM, int GTM, int BTW>
+template <int NBTM, int GTM, int BTW, int CH>
 __global__ void __launch_bounds__(NT, 1) dpg_adjoint_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
   const int tid = threadIdx.x;
   Ctx X;
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_adjoint_kernel(const __grid_constan
     __syncthreads();
     phase_b<BTW>(P, L, cell, X);
     __syncthreads();
-    phase_gram<GTM, 0>(P, L, cell, X);
+    phase_gram<GTM, CH>(P, L, cell, X);
     phase_factor(P, X);
     phase_adj_solve<NBTM>(P, L);
     phase_adj_p<NBTM>(P, L, cell);
@@ -394,14 +394,14 @@ __global__ void __launch_bounds__(NT, 1) dpg_adjoint_kernel(const __grid_constan
   }
 }
 
-#define DPG_ADJ_INSTANCES(X) X(12, 5, 4) X(16, 6, 4) X(20, 8, 4) X(24, 12, 6)
+#define DPG_ADJ_INSTANCES(X) X(12, 5, 4, 8) X(16, 6, 4, 8) X(20, 8, 4, 8) X(24, 12, 6, 8) X(24, 12, 6, 4)
 
 static KernelFn pick_adjoint_kernel(const DpgPlanDev* plan) {
   const int per = (plan->ngb + DPG_NWARPS - 1) / DPG_NWARPS;
   int btw = 0;
   for (int s = 0; s < plan->nseg; s++) btw = std::max(btw, (plan->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
-#define DPG_PICK(NB, GT, BT) \
-  if (plan->NBT <= NB && per <= GT && btw <= BT) return dpg_adjoint_kernel<NB, GT, BT>;
+#define DPG_PICK(NB, GT, BT, CH) \
+  if (plan->NBT <= NB && per <= GT && btw <= BT && plan->chg == CH) return dpg_adjoint_kernel<NB, GT, BT, CH>;
   DPG_ADJ_INSTANCES(DPG_PICK)
 #undef DPG_PICK
   return nullptr;

@@ -23,7 +23,7 @@ __device__ __forceinline__ void energy_residual(const DpgPlanDev& P, const DpgLa
   }
 }
 
-template <int NBTM, int GTM, int BTW>
+template <int NBTM, int GTM, int BTW, int CH>
 __global__ void __launch_bounds__(NT, 1) dpg_energy_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   Ctx X;
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_energy_kernel(const __grid_constant
     __syncthreads();
     energy_residual(P, L, cell);
     __syncthreads();
-    phase_gram<GTM, 0>(P, L, cell, X);
+    phase_gram<GTM, CH>(P, L, cell, X);
     phase_factor(P, X);
     phase_trsm<NBTM>(P, L, cell, X);
     // |L^-1 r|^2: row fcol of the W^T tiles of column tile fcol / 8
@@ -75,14 +75,17 @@ __global__ void __launch_bounds__(NT, 1) dpg_energy_kernel(const __grid_constant
   }
 }
 
-#define DPG_ENERGY_INSTANCES(X) X(12, 5, 4) X(16, 6, 4) X(20, 8, 4) X(24, 12, 6)
+// Gram points per chunk (CH) fixed at compile time, as in the assembly kernel; the
+// picker takes the first instance whose sizes and chunk length fit the plan.
+#define DPG_ENERGY_INSTANCES(X) \
+  X(12, 5, 4, 8) X(16, 6, 4, 8) X(20, 8, 4, 8) X(22, 9, 3, 8) X(24, 12, 6, 8) X(24, 12, 6, 4)
 
 static KernelFn pick_energy_kernel(const DpgPlanDev* plan) {
   const int per = (plan->ngb + DPG_NWARPS - 1) / DPG_NWARPS;
   int btw = 0;
   for (int s = 0; s < plan->nseg; s++) btw = std::max(btw, (plan->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
-#define DPG_PICK(NB, GT, BT) \
-  if (plan->NBT <= NB && per <= GT && btw <= BT) return dpg_energy_kernel<NB, GT, BT>;
+#define DPG_PICK(NB, GT, BT, CH) \
+  if (plan->NBT <= NB && per <= GT && btw <= BT && plan->chg == CH) return dpg_energy_kernel<NB, GT, BT, CH>;
   DPG_ENERGY_INSTANCES(DPG_PICK)
 #undef DPG_PICK
   return nullptr;
@@ -91,7 +94,7 @@ static KernelFn pick_energy_kernel(const DpgPlanDev* plan) {
 // DLS local matrices (TBF::localStiffnessMatrixAndRHS_DLS, BF.cpp:1169-1306: the
 // factored solve overwrites B and F in place): W = L^-1 B as (C, M, N) "trial x
 // test" and y = L^-1 F as (C, N), user numbering, L the unscaled Cholesky factor of G.
-template <int NBTM, int GTM, int BTW>
+template <int NBTM, int GTM, int BTW, int CH>
 __global__ void __launch_bounds__(NT, 1) dpg_dls_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
   const int tid = threadIdx.x;
   Ctx X;
@@ -111,7 +114,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_dls_kernel(const __grid_constant__ 
     __syncthreads();
     phase_b<BTW>(P, L, cell, X);
     __syncthreads();
-    phase_gram<GTM, 0>(P, L, cell, X);
+    phase_gram<GTM, CH>(P, L, cell, X);
     phase_factor(P, X);
     phase_trsm<NBTM>(P, L, cell, X);
     // W^T tile (J, I), element (r, c) = W[I*8 + c][J*8 + r]
@@ -144,8 +147,8 @@ static KernelFn pick_dls_kernel(const DpgPlanDev* plan) {
   const int per = (plan->ngb + DPG_NWARPS - 1) / DPG_NWARPS;
   int btw = 0;
   for (int s = 0; s < plan->nseg; s++) btw = std::max(btw, (plan->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
-#define DPG_PICK(NB, GT, BT) \
-  if (plan->NBT <= NB && per <= GT && btw <= BT) return dpg_dls_kernel<NB, GT, BT>;
+#define DPG_PICK(NB, GT, BT, CH) \
+  if (plan->NBT <= NB && per <= GT && btw <= BT && plan->chg == CH) return dpg_dls_kernel<NB, GT, BT, CH>;
   DPG_ENERGY_INSTANCES(DPG_PICK)
 #undef DPG_PICK
   return nullptr;

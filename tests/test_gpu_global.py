@@ -90,3 +90,41 @@ def test_entries_outside_the_graph_are_counted():
     torch.cuda.synchronize()
     assert int(missing.item()) > 0
     assert np.isfinite(vals.cpu().numpy()).all()
+
+
+def test_scatter_hex_conforming_map_matches_dense():
+    """The hex grid's conforming-shaped trace map (each trace point shared by the faces and
+    cells that touch it): the per-cell condensation onto distinct global dofs must give the
+    dense C^T S C accumulation."""
+    from camellia2_b200 import mesh
+    from tests.helpers import poisson3d
+    n = 3
+    form, bucket, nodes, par = poisson3d(2, 1, n, 0.1)
+    plan = dlib.Plan(bucket)
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, plan.info, C)
+    out = plan.assemble(*(torch.as_tensor(x).cuda() for x in (nodes, par, co)))
+    torch.cuda.synchronize()
+    S, s = out["S"].cpu().numpy(), out["s"].cpu().numpy()
+    t = S.shape[1]
+    g, ng = mesh.hex_trace_map(n, n, n, 2)
+    ptr = np.arange(C * t + 1, dtype=np.int64)
+    gid = g.reshape(-1)
+    w = np.ones(C * t)
+    A, b = _dense(S, s, ptr, gid, w, ng)
+    pattern = np.zeros((ng, ng), dtype=bool)
+    for c in range(C):
+        pattern[np.ix_(g[c], g[c])] = True
+    row_ptr, col = _graph(A, ~pattern)
+    dev = lambda x: torch.as_tensor(x).cuda()  # noqa: E731
+    vals = torch.zeros(col.shape[0], dtype=torch.float64, device="cuda")
+    rhs = torch.zeros(ng, dtype=torch.float64, device="cuda")
+    missing = dlib.scatter_global(dev(S), dev(s), dev(ptr), dev(gid), None, ng, dev(row_ptr), dev(col), vals, rhs)
+    torch.cuda.synchronize()
+    assert int(missing.item()) == 0
+    Ag = np.zeros((ng, ng))
+    v = vals.cpu().numpy()
+    for r in range(ng):
+        Ag[r, col[row_ptr[r]:row_ptr[r + 1]]] = v[row_ptr[r]:row_ptr[r + 1]]
+    assert np.linalg.norm(Ag - A) <= 1e-12 * np.linalg.norm(A)
+    assert np.linalg.norm(rhs.cpu().numpy() - b) <= 1e-12 * np.linalg.norm(b)

@@ -21,7 +21,8 @@ def _dev(x):
     return torch.as_tensor(np.ascontiguousarray(x)).cuda()
 
 
-@pytest.mark.parametrize("make", [lambda: poisson3d(2, 1, 2, 0.1), lambda: poisson2d(4, 2, 2, 2, 0.2)])
+@pytest.mark.parametrize("make", [lambda: poisson3d(2, 1, 2, 0.1), lambda: poisson2d(4, 2, 2, 2, 0.2),
+                                  lambda: poisson2d(2, 2, 80, 80, 0.2)])
 def test_recovered_fields_match_dense_solve(make):
     form, bucket, nodes, par = make()
     plan = dlib.Plan(bucket)
