@@ -261,10 +261,12 @@ int dpg_energy_error(dpg_plan* plan, int C, const double* nodes, const int8_t* p
  * sum_k map_w[k] x[map_gid[k]], k in [map_ptr[c t + a], map_ptr[c t + a + 1])
  * (map_w NULL: all weights 1).  Adds sum_c C_c^T S_c C_c into the values of the
  * caller's CSR graph (n_global rows; row_ptr, col_idx sorted within rows) and
- * sum_c C_c^T s_c into rhs (may be NULL); entries absent from the graph or with a
- * global index outside [0, n_global) are counted in *missing (device int) and
- * skipped.  S (C,t,t), s (C,t) as from dpg_assemble.  Device pointers;
- * summation order (atomics) varies between runs in the last bits. */
+ * sum_c C_c^T s_c into rhs (may be NULL); contributions whose target is absent from
+ * the graph or whose global index is outside [0, n_global) are skipped and *missing
+ * (device int) is raised by a positive count (0 when nothing was skipped).  S (C,t,t),
+ * s (C,t) as from dpg_assemble.  Its tables take 4 t^2 + 104 t + 12 bytes of shared
+ * memory per CTA, which must fit in 200 KB (t <= 213), else DPG_ERR_UNSUPPORTED.  Device pointers; the sum
+ * over cells runs through atomics, so its last bits vary between runs. */
 int dpg_scatter_global(int C, int t, const int64_t* map_ptr, const int64_t* map_gid, const double* map_w,
                        int64_t n_global, const int64_t* row_ptr, const int64_t* col_idx, const double* S,
                        const double* s, double* values, double* rhs, int* missing, void* stream);
