@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the other configurations' timings")
+    p.add_argument("--no-next", action="store_true",
+                   help="skip the timings of the kernels after the assembly (recovery, energy, DLS, scatter)")
     return p.parse_args()
 
 
@@ -150,16 +152,19 @@ def next_rows(torch, plan, info, n, d_nodes, d_par, d_co, out, peak_tflops, hbm_
     resident (CUDA events, 3 launches after one warm-up), each with its roofline."""
     from camellia2_b200 import lib, mesh
 
-    def timeit(fn, reps=3):
+    def timeit(fn, reps=5):
+        # median of single launches, after one warm-up
         fn()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        ts = []
         for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
             fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(statistics.median(ts))
 
     C, M, N, nf, nt = d_nodes.shape[0], info["M"], info["N"], info["n_field"], info["n_trace"]
     FG, FB, _, _ = flops_parts(N, M, nf, nt, info["Q_G"], info["Q_B"], info["Q_side"], info["n_sides"],
@@ -213,7 +218,25 @@ def next_rows(torch, plan, info, n, d_nodes, d_par, d_co, out, peak_tflops, hbm_
                              "bytes": by, "achieved_gbs": by / ms * 1e-6, "frac_of_measured_hbm": by / ms * 1e-6 / hbm_gbs,
                              "missing": int(miss[0].item()),
                              "map": "hex trace points identified by lattice position (50 global dofs per cell)"}
-    del vals, cols, row_ptr
+    # the same with the symbolic part done once (dpg_scatter_plan_*)
+    t0 = time.perf_counter()
+    splan = lib.ScatterPlan(C, nt, ptr, gflat, None, ng, row_ptr, cols)
+    torch.cuda.synchronize()
+    create_ms = (time.perf_counter() - t0) * 1e3
+
+    def scat_plan():
+        vals.zero_()
+        rhs.zero_()
+        splan.apply(out["S"], out["s"], vals, rhs)
+    ms = timeit(scat_plan)
+    gs = np.sort(gid_np, axis=1)
+    pairs = int((((gs[:, 1:] != gs[:, :-1]).sum(axis=1) + 1) ** 2).sum())
+    by = 8 * C * (nt * nt + nt) + 4 * pairs + 8 * nnz + 8 * ng
+    res["scatter_global_plan_apply"] = {"ms": ms, "cells_per_s": C / ms * 1e3, "bound": "hbm", "bytes": by,
+                                        "distinct_pairs": pairs, "achieved_gbs": by / ms * 1e-6,
+                                        "frac_of_measured_hbm": by / ms * 1e-6 / hbm_gbs,
+                                        "plan_create_ms_wall": create_ms, "missing": int(splan.missing.item())}
+    del splan, vals, cols, row_ptr
     torch.cuda.empty_cache()
     return res
 
@@ -491,8 +514,8 @@ def main():
             "parity_vs_oracle_max_rel": parity,
             "info_nonzero_cells": bad,
             "other_configs": None if args.no_extra else other_configs(torch),
-            "next_rows": None if args.no_extra else next_rows(torch, plan, info, n, d_nodes, d_par, d_co, out, peak,
-                                                              measured_hbm_gbs()),
+            "next_rows": None if args.no_next else next_rows(torch, plan, info, n, d_nodes, d_par, d_co, out, peak,
+                                                             measured_hbm_gbs()),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

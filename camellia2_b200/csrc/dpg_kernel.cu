@@ -1370,12 +1370,14 @@ __global__ void __launch_bounds__(256) recover_fields_kernel(int C, int M, int n
   }
 }
 
-// nf <= 32 and M <= 256: one warp per cell.  The nf leading rows of the cell's K (one
-// contiguous block) and its trace values are staged in a per-warp shared tile with
-// coalesced, independent loads; lane i then holds row i of the equilibrated K_ff in
-// registers and the Cholesky factorisation, both triangular solves and the unscaling run
-// on shuffles, without a block barrier.  Same results and info as the block kernel above.
-constexpr int RF_MAXW = 4;  // warps per block at most
+// nf <= 32: one warp per cell.  K_ff goes to a per-warp shared tile by 8-byte
+// asynchronous copies (all in flight at once); K_ft t is formed from coalesced reads of
+// the K_ft rows, each lane holding partial sums of all rows, which one butterfly
+// reduce-scatter (31 shuffles) turns into lane i's row sum.  Lane i then holds row i of
+// the equilibrated K_ff in registers and the Cholesky factorisation, both triangular
+// solves and the unscaling run on shuffles, without a block barrier.  Same results and
+// info as the block kernel above.
+constexpr int RF_MAXW = 1;  // warps per block
 
 __global__ void __launch_bounds__(RF_MAXW * 32) recover_fields_warp_kernel(int C, int M, int nf,
                                                                          const double* __restrict__ K,
@@ -1386,35 +1388,51 @@ __global__ void __launch_bounds__(RF_MAXW * 32) recover_fields_warp_kernel(int C
   extern __shared__ double rs[];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int ld = M + 1;                 // odd row stride: conflict-free column reads
-  double* st = rs + (size_t)warp * (nf * ld + M);
-  double* ts = st + nf * ld;            // trace values
+  constexpr int ld = 33;                // odd row stride: conflict-free column reads
+  double* st = rs + (size_t)warp * (32 * ld + M);
+  double* ts = st + 32 * ld;            // trace values
   const int nt = M - nf;
   for (int cell = blockIdx.x * nwarps + warp; cell < C; cell += gridDim.x * nwarps) {
     const double* Kc = K + (size_t)cell * M * M;
     const double* tc = t_in + (size_t)cell * nt;
-    // asynchronous 8-byte copies: every element of the block in flight at once
     for (int r = 0; r < nf; r++)
-      for (int c = lane; c < M; c += 32)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(st + r * ld + c)),
-                     "l"(Kc + (size_t)r * M + c)
+      if (lane < nf)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(st + r * ld + lane)),
+                     "l"(Kc + (size_t)r * M + lane)
                      : "memory");
     for (int j = lane; j < nt; j += 32)
       asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(ts + j)), "l"(tc + j) : "memory");
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    // partial sums of K_ft(i,:) t over this lane's columns, all rows
+    double p[32];
+#pragma unroll
+    for (int i = 0; i < 32; i++) p[i] = 0.0;
+    for (int c0 = 0; c0 < nt; c0 += 32) {
+      const int c = c0 + lane;
+      const double tv = c < nt ? tc[c] : 0.0;
+#pragma unroll
+      for (int i = 0; i < 32; i++)
+        if (i < nf && c < nt) p[i] += Kc[(size_t)i * M + nf + c] * tv;
+    }
+    // reduce-scatter: after the step with offset o a lane keeps the rows whose bit o
+    // matches its own; at the end lane i holds row i's sum in p[0]
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      const bool hi = (lane & o) != 0;
+#pragma unroll
+      for (int r = 0; r < o; r++) {
+        const double send = hi ? p[r] : p[r + o];
+        const double keep = hi ? p[r + o] : p[r];
+        p[r] = keep + __shfl_xor_sync(FULL, send, o);
+      }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncwarp();
     const int i = lane;
     double bi = 0.0, sc = 1.0;  // lane i: l_i - K_ft(i,:) t and s_i = K_ii^-1/2
     if (i < nf) {
-      const double* row = st + i * ld;
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      int j = 0;
-      for (; j + 4 <= nt; j += 4)
-#pragma unroll
-        for (int q = 0; q < 4; q++) acc[q] += row[nf + j + q] * ts[j + q];
-      for (; j < nt; j++) acc[0] += row[nf + j] * ts[j];
-      bi = l[(size_t)cell * M + i] - ((acc[0] + acc[1]) + (acc[2] + acc[3]));
-      const double d = row[i];
+      bi = l[(size_t)cell * M + i] - p[0];
+      const double d = st[i * ld + i];
       sc = d > 0.0 ? rsqrt(d) : 1.0;
     }
     // rows and columns nf..31 are padded with the identity, so every step below runs
@@ -1473,7 +1491,7 @@ __global__ void __launch_bounds__(RF_MAXW * 32) recover_fields_warp_kernel(int C
 int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const double* l, const double* t, double* u,
                               int32_t* info, cudaStream_t stream) {
   if (C <= 0) return DPG_OK;
-  const size_t per_warp = ((size_t)nf * (M + 1) + M) * sizeof(double);
+  const size_t per_warp = ((size_t)32 * 33 + M) * sizeof(double);
   if (nf <= 32 && per_warp <= 100 * 1024) {
     // one-warp blocks: as many resident per SM as the staging tiles allow
     static int wconfigured = 0;
@@ -1499,255 +1517,6 @@ int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const doubl
   }
   const int grid = std::min(C, (g_num_sms > 0 ? g_num_sms : 148) * 4);
   recover_fields_kernel<<<grid, 256, bytes, stream>>>(C, M, nf, K, l, t, u, info);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
-  return DPG_OK;
-}
-
-// Global assembly of the condensed cell matrices (GDAMinimumRule::interpretLocalData,
-// GDAMinimumRule.cpp:714-800, through LocalDofMapper's C, then the insertion into the
-// global system, Solution.cpp:1263-1293): values += sum_c C_c^T S_c C_c and
-// rhs += sum_c C_c^T s_c on a CSR graph the caller owns.  Local dof a of cell c
-// stands for sum_k w_k x[gid_k], k in [ptr[c t + a], ptr[c t + a + 1]).
-//
-// One CTA per cell.  The cell's map entries are ranked by global id, so C_c^T S_c C_c
-// is formed on the cell's distinct global dofs (a trace point shared by three faces of
-// a hex is one row, not three): each distinct (row, column) pair costs one atomic
-// instead of one per pair of local dofs.  The CSR row of each distinct dof is read
-// once, coalesced, and matched against the cell's sorted ids to find the targets.
-// Within a cell the sums have a fixed order; across cells the atomics make the last
-// bits depend on the order of arrival.  A cell with more map entries than the shared
-// tables hold goes through the per-entry path (binary search per local pair).
-namespace {
-__device__ __forceinline__ long long csr_find(const int64_t* __restrict__ row_ptr, const int64_t* __restrict__ col,
-                                              int64_t r, int64_t c) {
-  long long lo = row_ptr[r], hi = row_ptr[r + 1] - 1;
-  while (lo <= hi) {
-    const long long mid = (lo + hi) >> 1;
-    const int64_t v = col[mid];
-    if (v == c) return mid;
-    if (v < c) lo = mid + 1;
-    else hi = mid - 1;
-  }
-  return -1;
-}
-
-constexpr int SG_T = 256;
-
-// Shared tables of one cell: ecap map entries at most, at most t*t distinct pairs.
-struct SgTables {
-  int* pos;        // nu*nu: offset of (u, v) in CSR row ug[u], or -1
-  int64_t* ug;     // distinct in-range global ids, ascending
-  int64_t* rbeg;   // row_ptr[ug[u]]
-  int64_t* eg;     // entry global id
-  double* ew;      // entry weight
-  int* erow;       // entry local row
-  int* erank;      // entry's distinct index, -1 when out of range
-  int* efirst;     // 1 for the first entry of each in-range id
-  int* ufirst;     // entries of distinct u: elist[ufirst[u] .. ufirst[u+1])
-  int* elist;
-};
-
-__host__ __device__ inline size_t sg_smem_bytes(int t, int ecap) {
-  return (size_t)t * t * 4 + 8 + (size_t)ecap * (8 + 8 + 8 + 8) + (size_t)ecap * 4 * 4 + ((size_t)ecap + 1) * 4;
-}
-
-__device__ inline SgTables sg_tables(void* base, int t, int ecap) {
-  SgTables T;
-  char* p = (char*)base;
-  T.ug = (int64_t*)p; p += (size_t)ecap * 8;
-  T.rbeg = (int64_t*)p; p += (size_t)ecap * 8;
-  T.eg = (int64_t*)p; p += (size_t)ecap * 8;
-  T.ew = (double*)p; p += (size_t)ecap * 8;
-  T.pos = (int*)p; p += (size_t)t * t * 4 + 8;
-  T.erow = (int*)p; p += (size_t)ecap * 4;
-  T.erank = (int*)p; p += (size_t)ecap * 4;
-  T.efirst = (int*)p; p += (size_t)ecap * 4;
-  T.elist = (int*)p; p += (size_t)ecap * 4;
-  T.ufirst = (int*)p;
-  return T;
-}
-
-// The per-entry path of one cell (any number of map entries).
-__device__ void scatter_cell_entries(int c, int t, const int64_t* __restrict__ ptr, const int64_t* __restrict__ gid,
-                                     const double* __restrict__ w, int64_t n, const int64_t* __restrict__ row_ptr,
-                                     const int64_t* __restrict__ col, const double* __restrict__ S,
-                                     const double* __restrict__ sv, double* __restrict__ values,
-                                     double* __restrict__ rhs, int* __restrict__ missing) {
-  const int tt = t * t;
-  for (int ab = threadIdx.x; ab < tt; ab += blockDim.x) {
-    const int a = ab / t, b = ab - a * t;
-    const double sab = S[(size_t)c * tt + ab];
-    const long long ia = (long long)c * t + a, ib = (long long)c * t + b;
-    for (int64_t ka = ptr[ia]; ka < ptr[ia + 1]; ka++) {
-      const double wa = w ? w[ka] : 1.0;
-      for (int64_t kb = ptr[ib]; kb < ptr[ib + 1]; kb++) {
-        const int64_t r = gid[ka], cc = gid[kb];
-        const long long pos = (r >= 0 && r < n && cc >= 0 && cc < n) ? csr_find(row_ptr, col, r, cc) : -1;
-        if (pos < 0) { atomicAdd(missing, 1); continue; }
-        atomicAdd(values + pos, wa * (w ? w[kb] : 1.0) * sab);
-      }
-    }
-    if (b == 0 && sv && rhs)
-      for (int64_t ka = ptr[ia]; ka < ptr[ia + 1]; ka++)
-        if (gid[ka] >= 0 && gid[ka] < n) atomicAdd(rhs + gid[ka], (w ? w[ka] : 1.0) * sv[ia]);
-  }
-}
-
-__global__ void __launch_bounds__(SG_T) scatter_global_kernel(int C, int t, int ecap, const int64_t* __restrict__ ptr,
-                                                              const int64_t* __restrict__ gid,
-                                                              const double* __restrict__ w, int64_t n,
-                                                              const int64_t* __restrict__ row_ptr,
-                                                              const int64_t* __restrict__ col,
-                                                              const double* __restrict__ S,
-                                                              const double* __restrict__ sv,
-                                                              double* __restrict__ values, double* __restrict__ rhs,
-                                                              int* __restrict__ missing) {
-  extern __shared__ __align__(16) double sg_smem[];
-  const SgTables T = sg_tables(sg_smem, t, ecap);
-  __shared__ int s_nu, s_nin, s_miss;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = SG_T / 32;
-  const int tt = t * t;
-  for (int c = blockIdx.x; c < C; c += gridDim.x) {
-    const int64_t e0 = ptr[(size_t)c * t], ne64 = ptr[(size_t)c * t + t] - e0;
-    if (ne64 > ecap || ne64 < 0) {
-      scatter_cell_entries(c, t, ptr, gid, w, n, row_ptr, col, S, sv, values, rhs, missing);
-      continue;
-    }
-    const int ne = (int)ne64;
-    if (tid == 0) { s_nu = 0; s_nin = 0; s_miss = 0; }
-    for (int a = tid; a < t; a += SG_T)
-      for (int64_t k = ptr[(size_t)c * t + a]; k < ptr[(size_t)c * t + a + 1]; k++) {
-        const int e = (int)(k - e0);
-        T.eg[e] = gid[k];
-        T.ew[e] = w ? w[k] : 1.0;
-        T.erow[e] = a;
-      }
-    __syncthreads();
-    // first occurrences of the in-range ids
-    int my_first = 0, my_in = 0;
-    for (int e = tid; e < ne; e += SG_T) {
-      const int64_t g = T.eg[e];
-      const int in = g >= 0 && g < n;
-      int first = in;
-      for (int q = 0; q < e && first; q++) first = T.eg[q] != g;
-      T.efirst[e] = first;
-      my_first += first;
-      my_in += in;
-    }
-    if (my_first) atomicAdd(&s_nu, my_first);
-    if (my_in) atomicAdd(&s_nin, my_in);
-    __syncthreads();
-    const int nu = s_nu, nin = s_nin;
-    if ((long long)nu * nu > tt) {  // more distinct pairs than the table holds
-      scatter_cell_entries(c, t, ptr, gid, w, n, row_ptr, col, S, sv, values, rhs, missing);
-      __syncthreads();
-      continue;
-    }
-    // ranks among the distinct ids
-    for (int e = tid; e < ne; e += SG_T) {
-      const int64_t g = T.eg[e];
-      int rank = -1;
-      if (g >= 0 && g < n) {
-        rank = 0;
-        for (int f = 0; f < ne; f++) rank += T.efirst[f] && T.eg[f] < g;
-        if (T.efirst[e]) {
-          T.ug[rank] = g;
-          T.rbeg[rank] = row_ptr[g];
-        }
-      }
-      T.erank[e] = rank;
-    }
-    __syncthreads();
-    // entries grouped by distinct index (stable)
-    for (int e = tid; e < ne; e += SG_T) {
-      const int r = T.erank[e];
-      if (r < 0) continue;
-      int p = 0;
-      for (int f = 0; f < ne; f++) {
-        const int rf = T.erank[f];
-        p += rf >= 0 && (rf < r || (rf == r && f < e));
-      }
-      T.elist[p] = e;
-      if (T.efirst[e]) T.ufirst[r] = p;
-    }
-    if (tid == 0) T.ufirst[nu] = nin;
-    for (int e = tid; e < nu * nu; e += SG_T) T.pos[e] = -1;
-    __syncthreads();
-    // targets: each distinct row's CSR columns matched against the sorted ids
-    for (int u = warp; u < nu; u += nwarp) {
-      const int64_t r = T.ug[u];
-      const int64_t beg = T.rbeg[u], end = row_ptr[r + 1];
-      for (int64_t p = beg + lane; p < end; p += 32) {
-        const int64_t cc = col[p];
-        int lo = 0, hi = nu - 1;
-        while (lo <= hi) {
-          const int mid = (lo + hi) >> 1;
-          const int64_t v = T.ug[mid];
-          if (v == cc) { T.pos[u * nu + mid] = (int)(p - beg); break; }
-          if (v < cc) lo = mid + 1;
-          else hi = mid - 1;
-        }
-      }
-    }
-    __syncthreads();
-    // one atomic per distinct pair
-    int my_miss = 0;
-    for (int e = tid; e < nu * nu; e += SG_T) {
-      const int u = e / nu, v = e - u * nu;
-      const int off = T.pos[e];
-      if (off < 0) { my_miss++; continue; }
-      double acc = 0.0;
-      for (int i = T.ufirst[u]; i < T.ufirst[u + 1]; i++) {
-        const int ea = T.elist[i];
-        const double* Sa = S + (size_t)c * tt + (size_t)T.erow[ea] * t;
-        double racc = 0.0;
-        for (int j = T.ufirst[v]; j < T.ufirst[v + 1]; j++) {
-          const int eb = T.elist[j];
-          racc += T.ew[eb] * __ldg(Sa + T.erow[eb]);
-        }
-        acc += T.ew[ea] * racc;
-      }
-      atomicAdd(values + T.rbeg[u] + off, acc);
-    }
-    if (sv && rhs)
-      for (int u = tid; u < nu; u += SG_T) {
-        double acc = 0.0;
-        for (int i = T.ufirst[u]; i < T.ufirst[u + 1]; i++) {
-          const int ea = T.elist[i];
-          acc += T.ew[ea] * sv[(size_t)c * t + T.erow[ea]];
-        }
-        atomicAdd(rhs + T.ug[u], acc);
-      }
-    if (my_miss) atomicAdd(&s_miss, my_miss);
-    __syncthreads();
-    // out-of-range entries: every local pair they take part in is skipped
-    if (tid == 0) {
-      const int skipped = s_miss + (ne * ne - nin * nin);
-      if (skipped) atomicAdd(missing, skipped);
-    }
-  }
-}
-}  // namespace
-
-int dpg_launch_scatter_global(int C, int t, const int64_t* ptr, const int64_t* gid, const double* w,
-                              int64_t n_global, const int64_t* row_ptr, const int64_t* col, const double* S,
-                              const double* s, double* values, double* rhs, int* missing, cudaStream_t stream) {
-  if (C <= 0 || t <= 0) return DPG_OK;
-  const int ecap = 2 * t;
-  const size_t bytes = sg_smem_bytes(t, ecap);
-  if (bytes > 200 * 1024) return dpg::fail(DPG_ERR_UNSUPPORTED, "too many trace dofs per cell for the global scatter");
-  static int configured = 0;
-  if (!configured) {
-    cudaFuncSetAttribute(scatter_global_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    configured = 1;
-  }
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scatter_global_kernel, SG_T, bytes);
-  const int sms = g_num_sms > 0 ? g_num_sms : 148;
-  const int grid = (int)std::min<long long>(C, (long long)sms * std::max(1, per_sm));
-  scatter_global_kernel<<<grid, SG_T, bytes, stream>>>(C, t, ecap, ptr, gid, w, n_global, row_ptr, col, S, s, values,
-                                                       rhs, missing);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;

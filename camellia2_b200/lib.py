@@ -56,6 +56,9 @@ def load():
     L.dpg_energy_error.argtypes = [vp, i] + [vp] * 6 + [vp]
     L.dpg_assemble_dls.argtypes = [vp, i] + [vp] * 6 + [vp]
     L.dpg_scatter_global.argtypes = [i, i] + [vp] * 3 + [ct.c_int64] + [vp] * 8
+    L.dpg_scatter_plan_create.argtypes = [i, i] + [vp] * 3 + [ct.c_int64] + [vp] * 4 + [ct.POINTER(vp)]
+    L.dpg_scatter_plan_apply.argtypes = [vp] * 6
+    L.dpg_scatter_plan_destroy.argtypes = [vp]
     L.dpg_compose_map.argtypes = [i, i] + [vp] * 3 + [ct.c_int64] + [vp] * 6 + [ct.c_int64, ct.POINTER(ct.c_int64),
                                                                                vp, vp]
     L.dpg_graph_capture.argtypes = [i, vp, i, ct.POINTER(vp)]
@@ -306,3 +309,28 @@ def compose_map(C, t, map_ptr, map_gid, map_w, n_fine, p_row_ptr, p_col, p_val, 
     missing.zero_()
     _check(L.dpg_compose_map(C, t, *args, _ptr(out_ptr), _ptr(gid), _ptr(w), n.value, ct.byref(n), _ptr(missing), sp))
     return out_ptr, gid[:n.value], w[:n.value], missing
+
+
+class ScatterPlan:
+    """dpg_scatter_plan_*: the global scatter's symbolic part once (map and graph fixed),
+    then apply(S, s, values, rhs) per assembly.  `missing` (device int32) holds the
+    count of contributions the graph has no place for."""
+
+    def __init__(self, C, t, map_ptr, map_gid, map_w, n_global, row_ptr, col_idx, stream=None):
+        import torch
+        self.missing = torch.zeros((1,), dtype=torch.int32, device=map_ptr.device)
+        h = ct.c_void_p()
+        self._keep = (map_ptr, map_gid, map_w, row_ptr, col_idx)
+        _check(load().dpg_scatter_plan_create(C, t, _ptr(map_ptr), _ptr(map_gid), _ptr(map_w), int(n_global),
+                                              _ptr(row_ptr), _ptr(col_idx), _ptr(self.missing), _stream_ptr(stream),
+                                              ct.byref(h)))
+        self.h = h
+
+    def apply(self, S, s, values, rhs=None, stream=None):
+        _check(load().dpg_scatter_plan_apply(self.h, _ptr(S.contiguous()), _ptr(None if s is None else s.contiguous()),
+                                             _ptr(values), _ptr(rhs), _stream_ptr(stream)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _LIB is not None:
+            _LIB.dpg_scatter_plan_destroy(self.h)
+            self.h = None

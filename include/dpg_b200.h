@@ -43,6 +43,8 @@
  *   dpg_assemble_dls          TBF::localStiffnessMatrixAndRHS_DLS (src/ScratchPad/BF.cpp:1169-1306)
  *   dpg_scatter_global        GDAMinimumRule::interpretLocalData + global insertion
  *                             (src/Mesh/GDAMinimumRule.cpp:714-800, src/Solution/Solution.cpp:1263-1293)
+ *   dpg_scatter_plan_*        the same, split into a symbolic part (once per mesh) and
+ *                             a numeric part (per assembly)
  *   dpg_compose_map           GMGOperator::computeCoarseStiffnessMatrix's P^T A P, as
  *                             per-cell maps C_c P for dpg_scatter_global
  *                             (src/Solution/GMGOperator.cpp:173-366,420-773)
@@ -264,12 +266,32 @@ int dpg_energy_error(dpg_plan* plan, int C, const double* nodes, const int8_t* p
  * sum_c C_c^T s_c into rhs (may be NULL); contributions whose target is absent from
  * the graph or whose global index is outside [0, n_global) are skipped and *missing
  * (device int) is raised by a positive count (0 when nothing was skipped).  S (C,t,t),
- * s (C,t) as from dpg_assemble.  Its tables take 4 t^2 + 104 t + 12 bytes of shared
- * memory per CTA, which must fit in 200 KB (t <= 213), else DPG_ERR_UNSUPPORTED.  Device pointers; the sum
+ * s (C,t) as from dpg_assemble.  Its per-cell tables take 4 t^2 + 104 t + 12 bytes of
+ * shared memory, which must fit in 200 KB (t <= 213), else DPG_ERR_UNSUPPORTED.  Device pointers; the sum
  * over cells runs through atomics, so its last bits vary between runs. */
 int dpg_scatter_global(int C, int t, const int64_t* map_ptr, const int64_t* map_gid, const double* map_w,
                        int64_t n_global, const int64_t* row_ptr, const int64_t* col_idx, const double* S,
                        const double* s, double* values, double* rhs, int* missing, void* stream);
+
+/* The same global scatter split into a symbolic part, done once for a fixed mesh,
+ * map and graph, and a numeric part per assembly (nonlinear iterations, time steps).
+ * dpg_scatter_plan_create ranks every cell's map entries by global id, groups them and
+ * finds the CSR position of each of the cell's distinct (row, column) pairs, into
+ * device arrays the plan owns; contributions with no target in the graph or a global
+ * id outside [0, n_global) raise *missing (device int, may be NULL) here, once, by a
+ * positive count, and are skipped by every apply.  The call waits for the stream.
+ * dpg_scatter_plan_apply adds sum_c C_c^T S_c C_c into values and sum_c C_c^T s_c
+ * into rhs (s and rhs may be NULL), with the same arithmetic as dpg_scatter_global;
+ * S, s and the plan's map and graph must describe the same cells.  A cell's map
+ * entries must fit the plan's shared tables (48 bytes each, 200 KB in all), else
+ * DPG_ERR_UNSUPPORTED.  Device pointers. */
+typedef struct dpg_scatter_plan dpg_scatter_plan;
+int dpg_scatter_plan_create(int C, int t, const int64_t* map_ptr, const int64_t* map_gid, const double* map_w,
+                            int64_t n_global, const int64_t* row_ptr, const int64_t* col_idx, int* missing,
+                            void* stream, dpg_scatter_plan** out);
+int dpg_scatter_plan_apply(const dpg_scatter_plan* plan, const double* S, const double* s, double* values,
+                           double* rhs, void* stream);
+int dpg_scatter_plan_destroy(dpg_scatter_plan* plan);
 
 /* Local-to-coarse maps for a Galerkin multigrid coarse operator.  Replaces the
  * sparse triple product P^T A P of GMGOperator::computeCoarseStiffnessMatrix

@@ -128,3 +128,78 @@ def test_scatter_hex_conforming_map_matches_dense():
         Ag[r, col[row_ptr[r]:row_ptr[r + 1]]] = v[row_ptr[r]:row_ptr[r + 1]]
     assert np.linalg.norm(Ag - A) <= 1e-12 * np.linalg.norm(A)
     assert np.linalg.norm(rhs.cpu().numpy() - b) <= 1e-12 * np.linalg.norm(b)
+
+
+def _to_dense_csr(vals, row_ptr, col, n):
+    Ag = np.zeros((n, n))
+    v = vals.cpu().numpy()
+    for r in range(n):
+        Ag[r, col[row_ptr[r]:row_ptr[r + 1]]] = v[row_ptr[r]:row_ptr[r + 1]]
+    return Ag
+
+
+def test_scatter_plan_matches_dense_and_accumulates():
+    """dpg_scatter_plan_*: symbolic part once, numeric part twice (the values double)."""
+    S, s, ptr, gid, w, n = _setup(2)
+    C, t = S.shape[0], S.shape[1]
+    A, b = _dense(S, s, ptr, gid, w, n)
+    row_ptr, col = _graph(A)
+    dev = lambda x: torch.as_tensor(x).cuda()  # noqa: E731
+    plan = dlib.ScatterPlan(C, t, dev(ptr), dev(gid), dev(w), n, dev(row_ptr), dev(col))
+    vals = torch.zeros(col.shape[0], dtype=torch.float64, device="cuda")
+    rhs = torch.zeros(n, dtype=torch.float64, device="cuda")
+    plan.apply(dev(S), dev(s), vals, rhs)
+    torch.cuda.synchronize()
+    assert int(plan.missing.item()) == 0
+    assert np.linalg.norm(_to_dense_csr(vals, row_ptr, col, n) - A) <= 1e-12 * np.linalg.norm(A)
+    assert np.linalg.norm(rhs.cpu().numpy() - b) <= 1e-12 * np.linalg.norm(b)
+    plan.apply(dev(S), dev(s), vals, rhs)
+    torch.cuda.synchronize()
+    assert np.linalg.norm(_to_dense_csr(vals, row_ptr, col, n) - 2 * A) <= 1e-12 * np.linalg.norm(A)
+
+
+def test_scatter_plan_counts_missing_at_creation():
+    S, s, ptr, gid, w, n = _setup(1)
+    C, t = S.shape[0], S.shape[1]
+    A, b = _dense(S, s, ptr, gid, w, n)
+    drop = np.zeros((n, n), dtype=bool)
+    drop[0, :] = True
+    row_ptr, col = _graph(A, drop)
+    gid = gid.copy()
+    gid[0] = n + 5
+    dev = lambda x: torch.as_tensor(x).cuda()  # noqa: E731
+    plan = dlib.ScatterPlan(C, t, dev(ptr), dev(gid), dev(w), n, dev(row_ptr), dev(col))
+    vals = torch.zeros(col.shape[0], dtype=torch.float64, device="cuda")
+    plan.apply(dev(S), None, vals)
+    torch.cuda.synchronize()
+    assert int(plan.missing.item()) > 0
+    assert np.isfinite(vals.cpu().numpy()).all()
+
+
+def test_scatter_plan_hex_map_equals_one_shot():
+    from camellia2_b200 import mesh
+    from tests.helpers import poisson3d
+    n = 3
+    form, bucket, nodes, par = poisson3d(2, 1, n, 0.1)
+    p = dlib.Plan(bucket)
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, p.info, C)
+    out = p.assemble(*(torch.as_tensor(x).cuda() for x in (nodes, par, co)))
+    t = out["S"].shape[1]
+    g, ng = mesh.hex_trace_map(n, n, n, 2)
+    keys = np.unique((g[:, :, None] * ng + g[:, None, :]).reshape(-1))
+    row_ptr = np.zeros(ng + 1, dtype=np.int64)
+    np.add.at(row_ptr, keys // ng + 1, 1)
+    row_ptr, col = np.cumsum(row_ptr), (keys % ng).astype(np.int64)
+    dev = lambda x: torch.as_tensor(x).cuda()  # noqa: E731
+    ptr, gid = dev(np.arange(C * t + 1, dtype=np.int64)), dev(g.reshape(-1))
+    v1 = torch.zeros(col.shape[0], dtype=torch.float64, device="cuda")
+    r1 = torch.zeros(ng, dtype=torch.float64, device="cuda")
+    dlib.scatter_global(out["S"], out["s"], ptr, gid, None, ng, dev(row_ptr), dev(col), v1, r1)
+    plan = dlib.ScatterPlan(C, t, ptr, gid, None, ng, dev(row_ptr), dev(col))
+    v2, r2 = torch.zeros_like(v1), torch.zeros_like(r1)
+    plan.apply(out["S"], out["s"], v2, r2)
+    torch.cuda.synchronize()
+    assert int(plan.missing.item()) == 0
+    assert float((v1 - v2).abs().max()) <= 1e-13 * float(v1.abs().max())
+    assert float((r1 - r2).abs().max()) <= 1e-13 * float(r1.abs().max())
