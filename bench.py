@@ -190,6 +190,14 @@ def next_rows(torch, plan, info, n, d_nodes, d_par, d_co, out, peak_tflops, hbm_
     res["dls"] = {"ms": ms, "cells_per_s": C / ms * 1e3, "bound": "tensor", "flops_per_cell": fl,
                   "achieved_tflops": fl * C / ms * 1e-9, "frac_of_measured_fp64": fl * C / ms * 1e-9 / peak_tflops,
                   "out_bytes_per_cell": 8 * (M * N + N)}
+    # reverse mode: dJ/df per point for J = sum_c (r^T K r + g^T l)
+    rr = torch.rand((C, M), dtype=torch.float64, device=d_nodes.device, generator=g) - 0.5
+    Kbar = rr[:, :, None] * rr[:, None, :]
+    lbar = torch.rand((C, M), dtype=torch.float64, device=d_nodes.device, generator=g) - 0.5
+    ms = timeit(lambda: plan.adjoint(d_nodes, d_par, d_co, Kbar, lbar))
+    res["adjoint"] = {"ms": ms, "cells_per_s": C / ms * 1e3,
+                      "what": "dpg_assemble_adjoint: Gram, B, Cholesky, X = G^-1 [B | F] recomputed, pull-back to f"}
+    del Kbar, lbar, rr
     torch.cuda.empty_cache()
     # global scatter with the conforming-shaped trace map of the hex grid
     gid_np, ng = mesh.hex_trace_map(n, n, n, 2)

@@ -30,10 +30,16 @@ def _setup(which, nx, ny, seed=3):
     if which == "cdr":
         form = fm.ConvectionDiffusionReactionFormulation(2)
         bucket = form.bucket(abi.TOPO_QUAD, 3, 2)
+    elif which == "poisson3d":  # the hex bucket of the bench (load f per point)
+        form = fm.PoissonFormulation(3)
+        bucket = form.bucket(abi.TOPO_HEX, 2, 1)
     else:
         form = fm.PoissonFormulation(2)
         bucket = form.bucket(abi.TOPO_QUAD, 2, 2)
-    nodes, par = mesh.quad_grid(nx, ny, 0.15, seed=seed)
+    if which == "poisson3d":
+        nodes, par = mesh.hex_grid(nx, ny, 1, 0.1, seed=seed)
+    else:
+        nodes, par = mesh.quad_grid(nx, ny, 0.15, seed=seed)
     plan = dlib.Plan(bucket)
     C = nodes.shape[0]
     co = coeffs_for(bucket, plan.info, C, seed=seed)
@@ -53,7 +59,7 @@ def _gpu_grad(plan, nodes, par, co, r, g):
     return cbar.cpu().numpy()
 
 
-@pytest.mark.parametrize("which", ["cdr", "poisson"])
+@pytest.mark.parametrize("which", ["cdr", "poisson", "poisson3d"])
 def test_adjoint_matches_oracle_central_differences(which, oracle_mod):
     bucket, plan, nodes, par, co, r, g = _setup(which, 2, 1)
     orc = oracle_mod.OraclePlan(bucket)
