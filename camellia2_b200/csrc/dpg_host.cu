@@ -540,6 +540,50 @@ static Rule tri_rule(int degree) {
   return r;
 }
 
+// Tables and memory layout of the large-bucket kernel (dpg_big_kernel): the formation
+// entries of E (one per segment and term), the test vars of each IP row, the user -> device
+// trial map, the per-CTA workspace (Z, then the per-point factors) and shared memory.
+static int big_layout(HostPlan* P) {
+  DpgPlanDev& g = P->dev;
+  g.adj_ok = 0;
+  g.Zn = g.Np + g.Mp;
+  if (g.Np > 4096 || g.Zn > 6144) return fail(DPG_ERR_UNSUPPORTED, "bucket too large for the large-bucket kernel");
+  g.ldz = (g.Zn + 7) & ~7;
+  for (int r = 0; r < g.niprows; r++) {
+    g.ipmask[r] = 0;
+    for (int e = g.rowstart[r]; e < g.rowstart[r + 1]; e++) g.ipmask[r] |= 1 << (g.ipent[e].gslot >> 2);
+  }
+  int vrow = 0;
+  g.nbe = 0;
+  for (int sg = 0; sg < g.nseg; sg++)
+    for (int lt = 0; lt < g.seg[sg].nterm; lt++) {
+      g.be[g.nbe++] = make_int4(sg, lt, vrow, g.seg[sg].npts);
+      vrow += g.seg[sg].npts;
+    }
+  std::vector<int> u2d(g.M, 0);
+  for (int b = 0; b < g.ntrial; b++) {
+    const DpgTrialVar& tr = g.trial[b];
+    const int cnt = (tr.kind == DPG_VAR_FIELD) ? tr.ncomp * tr.card_comp : tr.per_side * g.ns;
+    for (int i = 0; i < cnt; i++) u2d[tr.user_off + i] = tr.dev_off + i;
+  }
+  g.u2d_trial = upload_i(P, u2d);
+  auto al = [](size_t x) { return (x + 31) & ~(size_t)31; };  // 256-byte aligned regions
+  size_t o = al((size_t)g.Zn * g.ldz);
+  g.bz_wq = (int)o; o += al(g.QGpad);
+  g.bz_bh = (int)o; o += al((size_t)g.QGpad * g.niprows * g.ntest * 4);
+  g.bz_vt = (int)o; o += al((size_t)vrow * 4);
+  g.bz_per_cta = o;
+  int s = 4 * 64 * 68;  // diagonal block, its inverse, two panel blocks (formation buffers alias them)
+  g.bs_sc = s; s += (g.Np + 15) & ~15;
+  g.bs_col = s; s += ((g.Np + 1) / 2 + 15) & ~15;
+  g.bs_int = s; s += 256;  // 512 ints: flags, chunk point maps, relevance lists
+  g.bs_nodes = s; s += 32;
+  g.bs_total = s;
+  if ((size_t)s * 8 > 232448) return fail(DPG_ERR_UNSUPPORTED, "large-bucket kernel: shared memory exceeded");
+  g.sm_total = s;
+  return DPG_OK;
+}
+
 static int build(HostPlan* P, const dpg_bucket_desc* D) {
   DpgPlanDev& g = P->dev;
   std::memset(&g, 0, sizeof(g));
@@ -646,8 +690,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   g.N = user_row;
   g.Np = dev_row;
   g.NBT = g.Np / 8;
-  if (g.NBT > DPG_MAX_NBT)
-    return fail(DPG_ERR_UNSUPPORTED, "test space too large for the single-CTA kernel (N > 192 after padding)");
+  if (g.NBT > DPG_MAX_NBT) g.big = 1;  // the large-bucket kernel
   // staged reference slots of all test vars at a list of volume-reference points
   auto fref_table = [&](const double* pts, int npts) {
     std::vector<double> out((size_t)npts * g.featstride, 0.0);
@@ -737,8 +780,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   g.fcol = g.nfp + g.ntp;
   g.Mp = g.fcol + 8;
   g.MBT = g.Mp / 8;
-  if (g.MBT > DPG_MAX_MBT)
-    return fail(DPG_ERR_UNSUPPORTED, "trial space too large for the single-CTA kernel (M > 120 after padding)");
+  if (g.MBT > DPG_MAX_MBT) g.big = 1;
   {
     int off = g.nfp;
     for (int b = 0; b < D->n_trial; b++) {
@@ -848,7 +890,8 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       if (!covered[u]) gz.push_back(u);
     g.ngz = (int)gz.size();
     g.gzero = upload_i(P, gz);
-    if ((g.ngb + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_GT) return fail(DPG_ERR_UNSUPPORTED, "too many G blocks");
+    if (!g.big && (g.ngb + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_GT)
+      return fail(DPG_ERR_UNSUPPORTED, "too many G blocks");
     void* p = nullptr;
     if (cudaMalloc(&p, tiles.size() * sizeof(DpgGTile)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
     cudaMemcpy(p, tiles.data(), tiles.size() * sizeof(DpgGTile), cudaMemcpyHostToDevice);
@@ -861,6 +904,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   std::vector<std::pair<int, DpgBTerm>> terms;  // (segment, term)
   std::vector<std::pair<int, DpgBTerm>> sterms; // (side, term): separable boundary terms
   auto separable = [&](int a, int op) {
+    if (g.big) return false;  // the large-bucket kernel integrates every side term by quadrature
     const int sp = g.test[a].space;
     return (sp == DPG_SPACE_HGRAD && op == DPG_OP_VALUE) || (sp == DPG_SPACE_HDIV && op == DPG_OP_DOT_NORMAL);
   };
@@ -959,7 +1003,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       const DpgBTerm& t = g.bterm[i];
       S.tvoff[lt] = tv;
       tv += t.ncol;
-      for (int J = t.col0 / 8; J <= (t.col0 + t.ncol - 1) / 8; J++) {
+      for (int J = t.col0 / 8; !g.big && J <= (t.col0 + t.ncol - 1) / 8; J++) {
         int k = -1;
         for (int kk = 0; kk < S.nblk; kk++)
           if (S.blk[kk].var == t.test_var && S.blk[kk].J == J) k = kk;
@@ -986,7 +1030,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       for (int I = V.ntile0; I < V.ntile0 + V.ntiles; I += 2) btiles.push_back(make_int4(I, S.blk[kb].J, kb, 0));
     }
     S.ntile = (int)btiles.size() - S.tile0;
-    if ((S.ntile + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_BTW)
+    if (!g.big && (S.ntile + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_BTW)
       return fail(DPG_ERR_UNSUPPORTED, "too many active B blocks in a segment");
     if (S.nterm == 0) continue;
     g.max_rec = std::max(g.max_rec, S.rec_len);
@@ -1011,7 +1055,8 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     // chunks are multiples of 4 points (one m16n8k16 k-step = 4 points x 4 slots)
     int ch = DPG_MAX_CHB;
     while (ch > 4 && !fits(ch)) ch -= 4;
-    if (!fits(ch)) return fail(DPG_ERR_UNSUPPORTED, "B-phase staging does not fit in shared memory");
+    if (g.big) ch = 1 << 20;  // no staging: one chunk per segment
+    else if (!fits(ch)) return fail(DPG_ERR_UNSUPPORTED, "B-phase staging does not fit in shared memory");
     for (int sg = 0; sg < g.nseg; sg++) {
       DpgSeg& S = g.seg[sg];
       if (S.nterm == 0) continue;
@@ -1191,8 +1236,12 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       else adj_terms_ok = false;  // a non-separable side term with a coefficient
     }
 
+  if (g.big) {
+    int rc = big_layout(P);
+    if (rc != DPG_OK) return rc;
+  }
   // ---- shared memory layout (doubles) ----------------------------------------
-  for (g.chg = DPG_CHG;; g.chg /= 2) {
+  for (g.chg = DPG_CHG; !g.big; g.chg /= 2) {
     auto al = [](int x) { return (x + 15) & ~15; };  // 128-byte aligned regions
     int o = 0;
     // Gram phase

@@ -1201,6 +1201,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_multi_kernel(const DpgPlanDev* __re
 }
 
 #include "dpg_energy.cuh"
+#include "dpg_big.cuh"
 
 typedef void (*MultiFn)(const DpgPlanDev*, const DpgLaunch*, const int*, int);
 #define DPG_MULTI_INSTANCES(X) X(16, 6, 4) X(24, 12, 6)
@@ -1224,7 +1225,43 @@ static int g_num_sms = 0;
 
 }  // namespace
 
+static int configure_big(const DpgPlanDev* plan) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t bytes = (size_t)plan->bs_total * sizeof(double);
+  if (optin > 0 && bytes > (size_t)optin) return dpg::fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
+  cudaError_t e = cudaFuncSetAttribute(dpg_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  if (g_num_sms == 0) {
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 1;
+  }
+  return DPG_OK;
+}
+
+// Large buckets: one CTA per SM, each with its own workspace (Z and the per-point factors).
+static int launch_big(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
+  if (Lin->parts || Lin->solve_only)
+    return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans support the assembly entry points only");
+  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  DpgLaunch L = *Lin;
+  void* ws = nullptr;
+  cudaError_t ea = cudaMallocAsync(&ws, (size_t)grid * plan->bz_per_cta * sizeof(double), stream);
+  if (ea != cudaSuccess) {
+    cudaGetLastError();
+    return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("workspace allocation: ") + cudaGetErrorString(ea));
+  }
+  L.scratch = (double*)ws;
+  dpg_big_kernel<<<grid, NT, (size_t)plan->bs_total * sizeof(double), stream>>>(*plan, L);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(ws, stream);
+  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DPG_OK;
+}
+
 int dpg_configure_kernels(const DpgPlanDev* plan) {
+  if (plan->big) return configure_big(plan);
   KernelFn k = pick_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
   // Several plans may share a kernel instance: the opt-in limit is the device's
@@ -1262,6 +1299,7 @@ int dpg_configure_kernels(const DpgPlanDev* plan) {
 int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const DpgLaunch* Lin, cudaStream_t stream) {
   (void)d_plan;
   if (Lin->C <= 0) return DPG_OK;
+  if (plan->big) return launch_big(plan, Lin, stream);
   KernelFn k = pick_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
   const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
@@ -1572,6 +1610,7 @@ int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_
 
 int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
   if (Lin->C <= 0) return DPG_OK;
+  if (plan->big) return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans support the assembly entry points only");
   KernelFn k = Lin->xsol ? pick_energy_kernel(plan) : pick_dls_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
   int dev = 0, optin = 0;
@@ -1606,6 +1645,8 @@ int dpg_launch_multi(const DpgPlanDev* hplans_in, const DpgLaunch* hl_in, int nb
   std::vector<int> cstart(nb + 1, 0);
   size_t stride = 0, smem = 0;
   for (int b = 0; b < nb; b++) {
+    if (hplans[b].big && hl[b].C > 0)
+      return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans run through dpg_assemble, not the multi-bucket launch");
     cstart[b + 1] = cstart[b] + std::max(0, hl[b].C);
     stride = std::max(stride, hplans[b].scratch_per_cta);
     smem = std::max(smem, (size_t)hplans[b].sm_total * sizeof(double));
@@ -1698,6 +1739,7 @@ double* g_noalloc_ptr[64] = {nullptr};  // device address of the array, per devi
 
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
   if (Lin->C <= 0) return DPG_OK;
+  if (plan->big) return dpg::fail(DPG_ERR_UNSUPPORTED, "dpg_assemble_noalloc: large-bucket plans need dpg_assemble");
   KernelFn k = pick_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
   if (plan->scratch_per_cta > DPG_NOALLOC_SCRATCH_DOUBLES)

@@ -194,4 +194,18 @@ struct DpgPlanDev {
   int a_sa, a_ldS;                                 // adjoint: S_A [MBT*8][a_ldS]
   int a_fs, a_xpf, a_ldx, a_geo, a_beta, a_cbar;   // adjoint pull-back
   size_t scratch_per_cta;                          // doubles of B scratch per CTA
+  // Large buckets (N > 192 or M > 120 after padding) run on dpg_big_kernel: per cell the
+  // lower triangle of Z = [[G, E], [E^T, 0]] (E = [B^T | F]; rows/columns: device test rows,
+  // then device trial columns) in a per-CTA global workspace.
+  int big;
+  int Zn, ldz;              // Z order (Np + Mp) and row stride (doubles)
+  int nbe;                  // E-formation entries, one per (segment, term)
+  int4 be[DPG_MAX_BF];      // (segment, segment-local term, first vt row, points)
+  int ipmask[DPG_MAX_IPROWS];  // test vars each IP row touches (bit a)
+  const int* u2d_trial;     // [M] user trial index -> device column
+  int bz_wq, bz_bh, bz_vt;  // per-CTA workspace after Z: w|J| at Gram points, per-point IP row
+                            // factors [QG][rows][ntest][4], per-point term factors [vt rows][4]
+  size_t bz_per_cta;        // doubles of per-CTA workspace
+  int bs_sc, bs_col, bs_int, bs_nodes, bs_total;  // shared memory (doubles): scales, column
+                                                  // records, ints, vertices; total
 };

@@ -1,0 +1,102 @@
+"""Large buckets (N > 192 or M > 120 after padding: the Stokes VGP quads p >= 3 and
+triangles p >= 4 of the uneven-cell workload, 2D Poisson k = 6, 3D Poisson k = 3) through
+the C-ABI against the CPU oracle on the same seeded inputs.
+
+Tolerance as in test_gpu_parity: relative Frobenius error <= 1e-12 per cell for K, l, S, s,
+or 5x the cell's measured FP64 floor (the change of K under random 1-ulp perturbations of G)
+where that floor exceeds 2e-13."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from camellia2_b200 import lib as dlib  # noqa: E402
+from tests.conftest import rel_fro  # noqa: E402
+from tests.helpers import coeffs_for, poisson2d, poisson3d, stokes2d, stokes_tri  # noqa: E402
+from tests.test_gpu_parity import fp64_floor  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "stokes2d_k3_dk2": lambda: stokes2d(3, 2, 2, 1, 0.1),       # N=228, M=119
+    "stokes2d_k4_dk2": lambda: stokes2d(4, 2, 2, 1, 0.1),       # N=315, M=184
+    "stokes2d_k5_dk2": lambda: stokes2d(5, 2, 1, 1, 0.1),       # N=416, M=263
+    "stokes2d_k6_dk2": lambda: stokes2d(6, 2, 1, 1, 0.1),       # N=531, M=356
+    "stokes_tri_k4_dk2": lambda: stokes_tri(4, 2, 1, 1, 0.1),   # N=180 (triangles)
+    "stokes_tri_k6_dk2": lambda: stokes_tri(6, 2, 1, 1, 0.1),   # N=295, M=225
+    "poisson2d_k6_dk1": lambda: poisson2d(6, 1, 2, 1, 0.2),     # N=176 but M=160: large by M
+    "poisson3d_k3_dk1": lambda: poisson3d(3, 1, 1, 0.1),        # N=365, M=258 (3D alternative)
+}
+
+
+def _dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a)).cuda()
+
+
+def _check(oracle_mod, o, ref, C):
+    assert (o["info"] == 0).all()
+    for c in range(C):
+        tol = 1e-12
+        errs = {k: rel_fro(o[k][c], ref[k][c]) for k in ("K", "l", "S", "s")}
+        if max(errs.values()) >= tol:
+            floor = fp64_floor(oracle_mod, ref["G"][c], ref["B"][c], ref["F"][c], ref["K"][c])
+            if floor > 2e-13:
+                tol = 5 * floor
+        for k, e in errs.items():
+            assert e < tol, (c, k, e, tol)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_big_bucket_matches_oracle(name, oracle_mod):
+    form, bucket, nodes, par = CASES[name]()
+    P = oracle_mod.OraclePlan(bucket)
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, P.info, C)
+    ref = P.assemble(nodes, par, co, parts=True)
+    plan = dlib.Plan(bucket)
+    assert plan.info == {**P.info, "precision": plan.info["precision"]}
+    out = plan.assemble(_dev(nodes), _dev(par), None if co is None else _dev(co))
+    torch.cuda.synchronize()
+    _check(oracle_mod, {k: v.cpu().numpy() for k, v in out.items()}, ref, C)
+
+
+def test_big_bucket_many_cells(oracle_mod):
+    """More cells than CTAs: every CTA reuses its workspace for several cells."""
+    form, bucket, nodes, par = stokes2d(3, 2, 20, 16, 0.15, seed=3)
+    P = oracle_mod.OraclePlan(bucket)
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, P.info, C)
+    ref = P.assemble(nodes, par, co, parts=True)
+    plan = dlib.Plan(bucket)
+    out = plan.assemble(_dev(nodes), _dev(par), _dev(co))
+    torch.cuda.synchronize()
+    _check(oracle_mod, {k: v.cpu().numpy() for k, v in out.items()}, ref, C)
+
+
+def test_big_bucket_host_api_and_flags(oracle_mod):
+    """Host buffers give the device call's results bit for bit; DPG_FLAG_NO_K returns S, s
+    alone and DPG_FLAG_NO_CONDENSE K, l alone, equal to the full call."""
+    form, bucket, nodes, par = stokes2d(4, 2, 2, 2, 0.1)
+    C = nodes.shape[0]
+    plan = dlib.Plan(bucket)
+    co = coeffs_for(bucket, plan.info, C)
+    d = plan.assemble(_dev(nodes), _dev(par), _dev(co))
+    torch.cuda.synchronize()
+    h = plan.assemble_host(nodes, par, co)
+    for k in ("K", "l", "S", "s", "info"):
+        assert np.array_equal(h[k], d[k].cpu().numpy()), k
+    for flags, kept in ((1, ("S", "s", "info")), (2, ("K", "l", "info"))):
+        part = {k: (np.empty_like(h[k]) if k in kept else None) for k in ("K", "l", "S", "s", "info")}
+        plan.assemble_host(nodes, par, co, out=part, flags=flags)
+        for k in kept:
+            assert np.array_equal(part[k], h[k]), (flags, k)
+
+
+def test_big_bucket_rejects_unsupported_entry_points():
+    """Entry points the large-bucket kernel does not provide fail with DPG_ERR_UNSUPPORTED."""
+    form, bucket, nodes, par = stokes2d(3, 2, 1, 1, 0.1)
+    plan = dlib.Plan(bucket)
+    co = coeffs_for(bucket, plan.info, 1)
+    with pytest.raises(dlib.DpgError) as ei:
+        plan.parts(_dev(nodes), _dev(par), _dev(co))
+    assert ei.value.code == 2
