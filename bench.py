@@ -135,7 +135,39 @@ def other_configs(torch):
         total += C
     ms = timeit(lambda: lib.assemble_multi(items))
     res["c3_stokes_quads_p1_2_tris_p1_3_multi"] = {"cells": total, "ms": ms, "cells_per_s": total / ms * 1e3}
+    del items
+    res["c3_stokes_forest_100k_graph"] = c3_forest(torch, timeit, dev)
     return res
+
+
+def c3_forest(torch, timeit, dev, total=100_000):
+    """The uneven-cell Stokes VGP workload: ~100k cells (70 % quads, 30 % triangles, p uniform
+    on 1..6, Delta p = 2, refinement level geometric on 0..4, jittered), twelve (topology, p)
+    buckets in one CUDA graph: the single-CTA buckets in one persistent launch, the large ones
+    (quads p >= 3, triangles p >= 4) on the large-bucket kernel after it.  Per-bucket device
+    times come from single-bucket launches."""
+    from camellia2_b200 import formulation as fm, lib, mesh
+    form = fm.StokesVGPFormulation(2)
+    items, keys, per = [], [], {}
+    for (topo, p), (nodes, par) in mesh.forest_buckets(total, seed=7).items():
+        pl = lib.Plan(form.bucket(topo, p, 2))
+        C = nodes.shape[0]
+        co = mesh.uniform_coeff(C, pl.info["n_slots"], pl.info["n_points_total"], seed=p)
+        items.append((pl, dev(nodes), dev(par), dev(co), pl.alloc_outputs(C)))
+        keys.append(("quad" if topo == 1 else "tri") + f"_p{p}")
+    for key, (pl, dn, dp, dc, out) in zip(keys, items):
+        C = dn.shape[0]
+        N, M = pl.info["N"], pl.info["M"]
+        ms = timeit(lambda: pl.assemble(dn, dp, dc, out=out), reps=1)
+        big = (N + 15) // 16 * 16 > 192 or M > 120
+        per[key] = {"cells": C, "N": N, "M": M, "ms": round(ms, 3), "cells_per_s": round(C / ms * 1e3),
+                    "kernel": "large-bucket" if big else "single-CTA"}
+    g = lib.Graph(items)
+    ms = timeit(g.launch, reps=2)
+    bad = sum(int((it[4]["info"] != 0).sum().item()) for it in items)
+    g.close()
+    n = sum(it[1].shape[0] for it in items)
+    return {"cells": n, "ms": ms, "cells_per_s": n / ms * 1e3, "info_nonzero_cells": bad, "buckets": per}
 
 
 def measured_hbm_gbs():

@@ -35,8 +35,8 @@ struct BigSm {
   double* Xi;  // [64][ZL] inverse of its factor
   double* LI;  // [64][ZL] L panel rows of the current row block
   double* LJ;  // [64][ZL] panel rows of the column block / staging of the raw panel
-  double* fa;  // [ZK][ZL] formation operand, tile rows (aliases D)
-  double* fb;  // [ZK][ZL] formation operand, tile columns (aliases D)
+  double* LJ1; // [64][ZL] second panel buffer (double buffering of the column blocks)
+  double* fa;  // [2][2][ZK][ZL] formation operands (rows, columns) x two chunks (aliases D)
   double* sc;  // [Np] equilibration scales
   int* col;    // [Np] test row record: var << 16 | local dof, or -1 (padding row)
   int* ints;   // [0] first failing G column, [1] first failing field column, [64..] relevance lists
@@ -50,8 +50,8 @@ __device__ __forceinline__ BigSm big_views(const DpgPlanDev& P) {
   S.Xi = sm + ZT * ZL;
   S.LI = sm + 2 * ZT * ZL;
   S.LJ = sm + 3 * ZT * ZL;
+  S.LJ1 = sm + 4 * ZT * ZL;
   S.fa = sm;
-  S.fb = sm + ZK * ZL;
   S.sc = sm + P.bs_sc;
   S.col = reinterpret_cast<int*>(sm + P.bs_col);
   S.ints = reinterpret_cast<int*>(sm + P.bs_int);
@@ -199,8 +199,11 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
   double acc[2][4];
 #pragma unroll
   for (int nb = 0; nb < 2; nb++) acc[nb][0] = acc[nb][1] = acc[nb][2] = acc[nb][3] = 0.0;
-  for (int k0 = 0; k0 < nk; k0 += ZK) {
-    // operands of this k-chunk: 2 sides x ZK x 64 values
+  // operands of k-chunk k0 (2 sides x ZK x 64 values) into buffer pair buf; chunk c + 1 is
+  // formed while the MMAs of chunk c run on the other pair, one barrier per chunk
+  auto operands = [&](int k0, int buf) {
+    double* const fa = S.fa + buf * 2 * ZK * ZL;
+    double* const fb = fa + ZK * ZL;
     for (int e = tid; e < 2 * ZK * ZT; e += NT) {
       const int side = e >> 10, kl = (e >> 6) & (ZK - 1), c = e & (ZT - 1);
       const int kk = k0 + kl;
@@ -242,10 +245,15 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
           }
         }
       }
-      (side ? S.fb : S.fa)[kl * ZL + c] = val;
+      (side ? fb : fa)[kl * ZL + c] = val;
     }
-    __syncthreads();
-    big_mma_kmajor(S.fa, S.fb, wr, wc, g, t, acc);
+  };
+  if (nk > 0) operands(0, 0);
+  __syncthreads();
+  for (int k0 = 0, c = 0; k0 < nk; k0 += ZK, c++) {
+    if (k0 + ZK < nk) operands(k0 + ZK, (c + 1) & 1);
+    const double* fa = S.fa + (c & 1) * 2 * ZK * ZL;
+    big_mma_kmajor(fa, fa + ZK * ZL, wr, wc, g, t, acc);
     __syncthreads();
   }
   const int ld = P.ldz;
@@ -360,18 +368,42 @@ __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, con
           *reinterpret_cast<double2*>(S.LI + r * ZL + c) = v;
           if (r < nri && c < w) *reinterpret_cast<double2*>(Z + (size_t)(ri0 + r) * ld + k0 + c) = v;
         }
+      // column blocks bj < bi come from the stored panel, double buffered through registers:
+      // tile bj + 1 is loaded while the MMAs of tile bj run; one barrier per tile
+      double pre[ZT * ZT / NT];
+      auto load_panel = [&](int bj) {
+        const int rj0 = rbeg + bj * ZT, nrj = min(ZT, Zn - rj0);
+#pragma unroll
+        for (int u = 0; u < ZT * ZT / NT; u++) {
+          const int e = tid + u * NT, r = e >> 6, c = e & (ZT - 1);
+          pre[u] = (r < nrj && c < w) ? Z[(size_t)(rj0 + r) * ld + k0 + c] : 0.0;
+        }
+      };
+      auto store_panel = [&](double* dst) {
+#pragma unroll
+        for (int u = 0; u < ZT * ZT / NT; u++) {
+          const int e = tid + u * NT;
+          dst[(e >> 6) * ZL + (e & (ZT - 1))] = pre[u];
+        }
+      };
+      if (bi > 0) {
+        load_panel(0);
+        store_panel(S.LJ1);
+      }
       __syncthreads();
       for (int bj = 0; bj <= bi; bj++) {
         const int rj0 = rbeg + bj * ZT, nrj = min(ZT, Zn - rj0);
-        const double* Lj = S.LI;
-        if (bj < bi) {
-          for (int e = tid; e < ZT * ZT; e += NT) {
-            const int r = e >> 6, c = e & (ZT - 1);
-            S.LJ[r * ZL + c] = (r < nrj && c < w) ? Z[(size_t)(rj0 + r) * ld + k0 + c] : 0.0;
+        const double* Lj = bj == bi ? S.LI : ((bj & 1) ? S.LJ : S.LJ1);
+        if (bj + 1 < bi) load_panel(bj + 1);
+        double2 zo[2][2];
+#pragma unroll
+        for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int r = wr + g + h * 8, c = wc + nb * 8 + 2 * t;
+            zo[nb][h] = (r < nri && c < nrj) ? *reinterpret_cast<const double2*>(Z + (size_t)(ri0 + r) * ld + rj0 + c)
+                                             : make_double2(0.0, 0.0);
           }
-          __syncthreads();
-          Lj = S.LJ;
-        }
 #pragma unroll
         for (int nb = 0; nb < 2; nb++) acc[nb][0] = acc[nb][1] = acc[nb][2] = acc[nb][3] = 0.0;
         big_mma_rows(S.LI, Lj, wk, wr, wc, g, t, acc);
@@ -380,14 +412,11 @@ __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, con
 #pragma unroll
           for (int h = 0; h < 2; h++) {
             const int r = wr + g + h * 8, c = wc + nb * 8 + 2 * t;
-            if (r < nri && c < nrj) {
-              double2* p = reinterpret_cast<double2*>(Z + (size_t)(ri0 + r) * ld + rj0 + c);
-              double2 v = *p;
-              v.x -= acc[nb][2 * h];
-              v.y -= acc[nb][2 * h + 1];
-              *p = v;
-            }
+            if (r < nri && c < nrj)
+              *reinterpret_cast<double2*>(Z + (size_t)(ri0 + r) * ld + rj0 + c) =
+                  make_double2(zo[nb][h].x - acc[nb][2 * h], zo[nb][h].y - acc[nb][2 * h + 1]);
           }
+        if (bj + 1 < bi) store_panel(((bj + 1) & 1) ? S.LJ : S.LJ1);
         __syncthreads();
       }
     }

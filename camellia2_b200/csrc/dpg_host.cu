@@ -573,7 +573,7 @@ static int big_layout(HostPlan* P) {
   g.bz_bh = (int)o; o += al((size_t)g.QGpad * g.niprows * g.ntest * 4);
   g.bz_vt = (int)o; o += al((size_t)vrow * 4);
   g.bz_per_cta = o;
-  int s = 4 * 64 * 68;  // diagonal block, its inverse, two panel blocks (formation buffers alias them)
+  int s = 5 * 64 * 68;  // diagonal block, its inverse, three panel blocks (formation buffers alias them)
   g.bs_sc = s; s += (g.Np + 15) & ~15;
   g.bs_col = s; s += ((g.Np + 1) / 2 + 15) & ~15;
   g.bs_int = s; s += 256;  // 512 ints: flags, chunk point maps, relevance lists
@@ -1674,12 +1674,36 @@ int dpg_recover_fields(dpg_plan* p, int C, const double* K, const double* l, con
   return dpg_launch_recover_fields(C, g.M, g.nf, K, l, trace_coeff, local_coeff, info, (cudaStream_t)stream);
 }
 
+// The buckets of a multi-bucket call: the single-CTA ones stay in (plans, ls) for one
+// persistent launch; the large ones move to (bp, bl) and follow on the same stream, one
+// launch of the large-bucket kernel each.
+static void split_big(std::vector<DpgPlanDev>& plans, std::vector<DpgLaunch>& ls, std::vector<DpgPlanDev>& bp,
+                      std::vector<DpgLaunch>& bl) {
+  std::vector<DpgPlanDev> sp;
+  std::vector<DpgLaunch> sl;
+  for (size_t i = 0; i < plans.size(); i++) {
+    if (plans[i].big) {
+      bp.push_back(plans[i]);
+      bl.push_back(ls[i]);
+    } else {
+      sp.push_back(plans[i]);
+      sl.push_back(ls[i]);
+    }
+  }
+  plans.swap(sp);
+  ls.swap(sl);
+}
+
 int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags) {
-  std::vector<DpgPlanDev> plans;
-  std::vector<DpgLaunch> ls;
+  std::vector<DpgPlanDev> plans, bp;
+  std::vector<DpgLaunch> ls, bl;
   int rc = multi_args(n_buckets, buckets, flags, plans, ls);
-  if (rc != DPG_OK || plans.empty()) return rc;
-  return dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), (cudaStream_t)stream, nullptr);
+  if (rc != DPG_OK) return rc;
+  split_big(plans, ls, bp, bl);
+  if (!plans.empty()) rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), (cudaStream_t)stream, nullptr);
+  for (size_t i = 0; rc == DPG_OK && i < bp.size(); i++)
+    if (bl[i].C > 0) rc = dpg_launch_assemble(&bp[i], nullptr, &bl[i], (cudaStream_t)stream);
+  return rc;
 }
 
 struct dpg_graph {
@@ -1687,33 +1711,50 @@ struct dpg_graph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int device = 0;
+  void* big_ws = nullptr;  // workspace of the large-bucket launches (they run one after another)
 };
 
 int dpg_graph_capture(int n_buckets, const dpg_bucket_batch* buckets, int flags, dpg_graph** out) {
   if (!out) return fail(DPG_ERR_INVALID_ARGUMENT, "null output handle");
   *out = nullptr;
-  std::vector<DpgPlanDev> plans;
-  std::vector<DpgLaunch> ls;
+  std::vector<DpgPlanDev> plans, bp;
+  std::vector<DpgLaunch> ls, bl;
   int rc = multi_args(n_buckets, buckets, flags, plans, ls);
   if (rc != DPG_OK) return rc;
-  if (plans.empty()) return fail(DPG_ERR_INVALID_ARGUMENT, "no cells to capture");
+  split_big(plans, ls, bp, bl);
+  size_t big_bytes = 0;
+  for (size_t i = 0; i < bp.size(); i++)
+    if (bl[i].C > 0) big_bytes = std::max(big_bytes, dpg_big_workspace_bytes(&bp[i], bl[i].C));
+  if (plans.empty() && big_bytes == 0) return fail(DPG_ERR_INVALID_ARGUMENT, "no cells to capture");
   dpg_graph* G = new dpg_graph();
   std::memset(&G->dev, 0, sizeof(G->dev));
   cudaGetDevice(&G->device);
-  G->dev.bytes = dpg_multi_bytes(plans.data(), ls.data(), (int)plans.size());
-  if (cudaMalloc(&G->dev.base, G->dev.bytes) != cudaSuccess) {
-    cudaGetLastError();
-    delete G;
-    return fail(DPG_ERR_OUT_OF_MEMORY, "graph workspace");
+  if (!plans.empty()) {
+    G->dev.bytes = dpg_multi_bytes(plans.data(), ls.data(), (int)plans.size());
+    if (cudaMalloc(&G->dev.base, G->dev.bytes) != cudaSuccess) {
+      cudaGetLastError();
+      delete G;
+      return fail(DPG_ERR_OUT_OF_MEMORY, "graph workspace");
+    }
+    rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), nullptr, &G->dev);
   }
-  rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), nullptr, &G->dev);
+  if (rc == DPG_OK && big_bytes > 0 && cudaMalloc(&G->big_ws, big_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    G->big_ws = nullptr;
+    rc = fail(DPG_ERR_OUT_OF_MEMORY, "graph workspace of the large buckets");
+  }
   cudaStream_t cs = nullptr;
   if (rc == DPG_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
     rc = fail(DPG_ERR_CUDA, "stream creation");
   if (rc == DPG_OK) {
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      rc = dpg_launch_multi_prepared(&G->dev, cs);
+      if (!plans.empty()) rc = dpg_launch_multi_prepared(&G->dev, cs);
+      for (size_t i = 0; rc == DPG_OK && i < bp.size(); i++) {
+        if (bl[i].C <= 0) continue;
+        bl[i].scratch = (double*)G->big_ws;
+        rc = dpg_launch_assemble(&bp[i], nullptr, &bl[i], cs);
+      }
       cudaError_t e2 = cudaStreamEndCapture(cs, &G->graph);
       if (rc == DPG_OK && e2 != cudaSuccess) rc = fail(DPG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e2));
     } else {
@@ -1744,6 +1785,7 @@ int dpg_graph_destroy(dpg_graph* G) {
   if (G->exec) cudaGraphExecDestroy(G->exec);
   if (G->graph) cudaGraphDestroy(G->graph);
   if (G->dev.base) cudaFree(G->dev.base);
+  if (G->big_ws) cudaFree(G->big_ws);
   delete G;
   return DPG_OK;
 }

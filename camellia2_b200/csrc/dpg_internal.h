@@ -50,6 +50,7 @@ int dpg_host_pipeline(const DpgPlanDev* plan, const DpgPlanDev* d_plan, void** d
                       cudaStream_t* streams, int C, const double* nodes, const int8_t* parity, const double* coeff,
                       double* K, double* l, double* S, double* s, int32_t* info, int flags);
 int dpg_make_solve_plan(int N, int M, DpgPlanDev* out);
+size_t dpg_big_workspace_bytes(const DpgPlanDev* plan, int C);  // large buckets: workspace of one launch
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);
 int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* L, cudaStream_t stream);

@@ -1229,13 +1229,23 @@ static int configure_big(const DpgPlanDev* plan) {
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const size_t bytes = (size_t)plan->bs_total * sizeof(double);
+  size_t bytes = (size_t)plan->bs_total * sizeof(double);
   if (optin > 0 && bytes > (size_t)optin) return dpg::fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
+  // every large plan shares the kernel: opt in to the device maximum so that configuring one
+  // plan never lowers the limit another plan needs
+  if (optin > 0) bytes = (size_t)optin;
   cudaError_t e = cudaFuncSetAttribute(dpg_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   if (g_num_sms == 0) {
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
     if (g_num_sms <= 0) g_num_sms = 1;
+    // keep freed stream-ordered workspaces in the pool between calls
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
   }
   return DPG_OK;
 }
@@ -1247,17 +1257,24 @@ static int launch_big(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t
   const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
   DpgLaunch L = *Lin;
   void* ws = nullptr;
-  cudaError_t ea = cudaMallocAsync(&ws, (size_t)grid * plan->bz_per_cta * sizeof(double), stream);
-  if (ea != cudaSuccess) {
-    cudaGetLastError();
-    return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("workspace allocation: ") + cudaGetErrorString(ea));
+  if (!L.scratch) {  // a caller-provided workspace holds dpg_big_workspace_bytes(plan, C)
+    cudaError_t ea = cudaMallocAsync(&ws, (size_t)grid * plan->bz_per_cta * sizeof(double), stream);
+    if (ea != cudaSuccess) {
+      cudaGetLastError();
+      return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("workspace allocation: ") + cudaGetErrorString(ea));
+    }
+    L.scratch = (double*)ws;
   }
-  L.scratch = (double*)ws;
   dpg_big_kernel<<<grid, NT, (size_t)plan->bs_total * sizeof(double), stream>>>(*plan, L);
   cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(ws, stream);
+  if (ws) cudaFreeAsync(ws, stream);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
+}
+
+size_t dpg_big_workspace_bytes(const DpgPlanDev* plan, int C) {
+  const int grid = std::min(std::max(C, 1), g_num_sms > 0 ? g_num_sms : 148);
+  return (size_t)grid * plan->bz_per_cta * sizeof(double);
 }
 
 int dpg_configure_kernels(const DpgPlanDev* plan) {

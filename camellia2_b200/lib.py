@@ -248,7 +248,8 @@ def _batches(items):
 
 
 def assemble_multi(items, stream=None, flags=0):
-    """dpg_assemble_multi: several buckets in one persistent launch."""
+    """dpg_assemble_multi: several buckets in one call; the single-CTA buckets share one
+    persistent launch, the large buckets follow on the same stream."""
     arr = _batches(items)
     _check(load().dpg_assemble_multi(len(items), ct.cast(arr, ct.c_void_p), _stream_ptr(stream), flags))
 

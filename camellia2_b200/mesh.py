@@ -153,3 +153,41 @@ def cdr_coeff(C, info, seed=1):
     co[:, 3] = rng.uniform(0.0, 1.0, size=(C, P))
     co[:, 4] = rng.uniform(-1.0, 1.0, size=(C, P))
     return co
+
+
+def forest_buckets(total=100_000, quad_frac=0.7, p_max=6, max_level=4, base_n=16, jitter=0.1, seed=1):
+    """Cells of the uneven-cell Stokes workload as a synthetic refined forest.
+
+    Each cell is a quad with probability quad_frac, else a triangle; its degree p is uniform
+    on 1..p_max and its refinement level L is drawn from a geometric law (P(L) ~ 2^-L)
+    truncated to 0..max_level.  A level-L cell of a base_n x base_n coarse grid of the unit
+    square has size h = 1 / (base_n 2^L); it sits at a random position of the grid of its level
+    and its vertices are jittered by U[-jitter h, jitter h].  The per-cell outputs depend on a
+    neighbour only through the side parity, so cells are generated independently with random
+    parities +-1 on their sides (hanging nodes change the global map, not the local matrices).
+
+    Returns {(topology, p): (nodes (C, nv, 2), parity (C, nv) int8)} with topology 1 = quad,
+    3 = triangle, and the cell counts in a deterministic order."""
+    rng = np.random.default_rng(seed)
+    is_quad = rng.uniform(size=total) < quad_frac
+    p = rng.integers(1, p_max + 1, size=total)
+    w = 0.5 ** np.arange(max_level + 1)
+    level = rng.choice(max_level + 1, size=total, p=w / w.sum())
+    out = {}
+    for topo, nv, ref in ((1, 4, np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]])),
+                          (3, 3, np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]]))):
+        for pp in range(1, p_max + 1):
+            sel = np.nonzero((is_quad == (topo == 1)) & (p == pp))[0]
+            C = len(sel)
+            if C == 0:
+                continue
+            n = base_n * 2 ** level[sel]
+            h = 1.0 / n
+            i = rng.integers(0, n)
+            j = rng.integers(0, n)
+            origin = np.stack([i * h, j * h], axis=-1)
+            nodes = origin[:, None, :] + h[:, None, None] * ref[None, :, :]
+            nodes = nodes + rng.uniform(-jitter, jitter, size=nodes.shape) * h[:, None, None]
+            par = np.where(rng.uniform(size=(C, nv)) < 0.5, -1, 1).astype(np.int8)
+            out[(topo, pp)] = (np.ascontiguousarray(nodes), par)
+    return out

@@ -100,3 +100,40 @@ def test_big_bucket_rejects_unsupported_entry_points():
     with pytest.raises(dlib.DpgError) as ei:
         plan.parts(_dev(nodes), _dev(par), _dev(co))
     assert ei.value.code == 2
+
+
+def _mixed_buckets():
+    """Single-CTA and large Stokes VGP buckets together (quads p = 2, 3, 5; triangles p = 3, 6)."""
+    out = []
+    for make, seed in ((lambda: stokes2d(2, 2, 2, 2, 0.1), 1), (lambda: stokes2d(3, 2, 3, 2, 0.1), 2),
+                       (lambda: stokes_tri(3, 2, 2, 1, 0.1), 3), (lambda: stokes2d(5, 2, 2, 1, 0.1), 4),
+                       (lambda: stokes_tri(6, 2, 1, 1, 0.1), 5)):
+        form, bucket, nodes, par = make()
+        plan = dlib.Plan(bucket)
+        co = coeffs_for(bucket, plan.info, nodes.shape[0], seed=seed)
+        out.append((plan, _dev(nodes), _dev(par), _dev(co)))
+    return out
+
+
+def test_multi_and_graph_with_large_buckets():
+    """dpg_assemble_multi and a captured graph over single-CTA and large buckets reproduce
+    dpg_assemble bucket by bucket, bit for bit, also after new coefficients are written into
+    the captured buffers."""
+    bs = _mixed_buckets()
+    refs = [p.assemble(n, q, c) for p, n, q, c in bs]
+    items = [(p, n, q, c, {k: v.fill_(7) for k, v in p.alloc_outputs(n.shape[0]).items()}) for p, n, q, c in bs]
+    dlib.assemble_multi(items)
+    torch.cuda.synchronize()
+    for (p, n, q, c, out), ref in zip(items, refs):
+        for k in ("K", "l", "S", "s", "info"):
+            assert torch.equal(out[k], ref[k]), k
+    g = dlib.Graph(items)
+    for p, n, q, c, out in items:
+        c.mul_(1.5).add_(0.1)
+    g.launch()
+    torch.cuda.synchronize()
+    for p, n, q, c, out in items:
+        ref = p.assemble(n, q, c)
+        for k in ("K", "l", "S", "s", "info"):
+            assert torch.equal(out[k], ref[k]), k
+    g.close()
