@@ -78,24 +78,38 @@ __device__ __forceinline__ void big_mma_kmajor(const double* fa, const double* f
   }
 }
 
-// acc += A B^T over k in [0, kn) (kn a multiple of 16), both stored row-major [row][k].
+// acc += A B^T over k in [0, kn) (kn a multiple of 16), both stored row-major [row][k].  Odd
+// k-steps go to a second set of accumulators, so four independent DMMA chains are in flight.
 __device__ __forceinline__ void big_mma_rows(const double* A, const double* B, int kn, int wr, int wc, int g, int t,
                                              double (&acc)[2][4]) {
-  for (int k0 = 0; k0 < kn; k0 += 16) {
-    double a[8];
+  double acc2[2][4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      a[2 * i] = A[(wr + g) * ZL + k0 + t + 4 * i];
-      a[2 * i + 1] = A[(wr + g + 8) * ZL + k0 + t + 4 * i];
-    }
+  for (int nb = 0; nb < 2; nb++) acc2[nb][0] = acc2[nb][1] = acc2[nb][2] = acc2[nb][3] = 0.0;
+  for (int k0 = 0; k0 < kn; k0 += 32) {
 #pragma unroll
-    for (int nb = 0; nb < 2; nb++) {
-      double b[4];
+    for (int half = 0; half < 2; half++) {
+      const int kk = k0 + 16 * half;
+      if (kk < kn) {
+        double a[8];
 #pragma unroll
-      for (int i = 0; i < 4; i++) b[i] = B[(wc + nb * 8 + g) * ZL + k0 + t + 4 * i];
-      dmma16(acc[nb], a, b);
+        for (int i = 0; i < 4; i++) {
+          a[2 * i] = A[(wr + g) * ZL + kk + t + 4 * i];
+          a[2 * i + 1] = A[(wr + g + 8) * ZL + kk + t + 4 * i];
+        }
+#pragma unroll
+        for (int nb = 0; nb < 2; nb++) {
+          double b[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) b[i] = B[(wc + nb * 8 + g) * ZL + kk + t + 4 * i];
+          dmma16(half ? acc2[nb] : acc[nb], a, b);
+        }
+      }
     }
   }
+#pragma unroll
+  for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+    for (int e = 0; e < 4; e++) acc[nb][e] += acc2[nb][e];
 }
 
 // Test vars whose (padded) rows meet [r0, r0 + 64).
@@ -406,13 +420,15 @@ __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, con
           }
 #pragma unroll
         for (int nb = 0; nb < 2; nb++) acc[nb][0] = acc[nb][1] = acc[nb][2] = acc[nb][3] = 0.0;
-        big_mma_rows(S.LI, Lj, wk, wr, wc, g, t, acc);
+        // on the diagonal tile, warp tiles wholly above the diagonal are not needed
+        const bool upper = bj == bi && wc >= wr + 16;
+        if (!upper) big_mma_rows(S.LI, Lj, wk, wr, wc, g, t, acc);
 #pragma unroll
         for (int nb = 0; nb < 2; nb++)
 #pragma unroll
           for (int h = 0; h < 2; h++) {
             const int r = wr + g + h * 8, c = wc + nb * 8 + 2 * t;
-            if (r < nri && c < nrj)
+            if (!upper && r < nri && c < nrj)
               *reinterpret_cast<double2*>(Z + (size_t)(ri0 + r) * ld + rj0 + c) =
                   make_double2(zo[nb][h].x - acc[nb][2 * h], zo[nb][h].y - acc[nb][2 * h + 1]);
           }

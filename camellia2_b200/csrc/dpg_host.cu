@@ -203,8 +203,8 @@ static int card_hdiv(int dim, int n) { return dim == 2 ? 2 * n * (n + 1) : 3 * n
 // optimized alpha table); the Lagrange functions are built through the
 // orthonormal PKD (Dubiner) polynomials, whose Vandermonde matrix on the lattice
 // is well conditioned.  RT_n uses the modal basis (p,0), (0,p) for p in P_{n-1}
-// and x h for homogeneous h of degree n-1: only the span of a test space enters
-// K, l and S.
+// and x psi for the orthonormal PKD polynomials psi of exact degree n-1 (a
+// well-conditioned choice): only the span of a test space enters K, l and S.
 // ----------------------------------------------------------------------------
 
 // Orthonormal Jacobi polynomial P_n^{(a,b)} on [-1,1].
@@ -366,11 +366,14 @@ static int tab_hdiv_tri(int n, const double* xi, double* out) {
       out[dof * 3 + 1] = c == 1 ? pv[k] : 0.0;
       out[dof * 3 + 2] = 2 * (c == 0 ? pr[k] : ps[k]);
     }
+  // x psi for the PKD polynomials psi of exact degree n-1: their leading homogeneous parts span
+  // the homogeneous polynomials of degree n-1, and unlike monomials they stay well conditioned
   for (int j = 0; j < n; j++, dof++) {
-    const double h = std::pow(xi[0], n - 1 - j) * std::pow(xi[1], j);
-    out[dof * 3] = xi[0] * h;
-    out[dof * 3 + 1] = xi[1] * h;
-    out[dof * 3 + 2] = (n + 1) * h;
+    double v, dr, ds;
+    pkd(n - 1 - j, j, 2 * xi[0] - 1, 2 * xi[1] - 1, v, dr, ds);
+    out[dof * 3] = xi[0] * v;
+    out[dof * 3 + 1] = xi[1] * v;
+    out[dof * 3 + 2] = 2 * v + 2 * (xi[0] * dr + xi[1] * ds);  // div(x psi) = 2 psi + x . grad psi
   }
   return dof;
 }
@@ -660,6 +663,28 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   };
 
   // ---- test vars ----------------------------------------------------------
+  // Large buckets (more than 192 test rows or 120 trial columns after padding) run on the
+  // large-bucket kernel, whose tiles need test vars padded to 8 rows only (the single-CTA
+  // kernel's 16 x 8 blocks need 16).
+  bool big_pre = false;
+  {
+    int np16 = 0, nf = 0, nt = 0;
+    for (int a = 0; a < D->n_test; a++) {
+      const dpg_var_desc& V = D->test[a];
+      const int c = V.space == DPG_SPACE_HGRAD ? card_hgrad_t(topo, d, V.poly_order)
+                                               : card_hdiv_t(topo, d, std::max(V.poly_order, 1));
+      np16 += (c + 15) & ~15;
+    }
+    for (int b = 0; b < D->n_trial; b++) {
+      const dpg_var_desc& V = D->trial[b];
+      if (V.kind == DPG_VAR_FIELD)
+        nf += (V.space == DPG_SPACE_VECTOR_HVOL ? d : 1) * card_hgrad_t(topo, d, std::max(V.poly_order - 1, 0));
+      else
+        nt += card_hgrad(d - 1, std::max(V.space == DPG_SPACE_HGRAD ? V.poly_order : V.poly_order - 1, 0)) * T.ns;
+    }
+    big_pre = np16 / 8 > DPG_MAX_NBT || (pad8(nf) + pad8(nt) + 8) / 8 > DPG_MAX_MBT;
+  }
+  if (big_pre) g.big = 1;
   int dev_row = 0, user_row = 0, foff = 0;
   std::vector<int> test_n(D->n_test);
   for (int a = 0; a < D->n_test; a++) {
@@ -674,7 +699,7 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
       tv.card = card_hdiv_t(topo, d, n);
     } else return fail(DPG_ERR_INVALID_ARGUMENT, "test vars must be HGRAD or HDIV");
     // rows padded to pairs of 8-row tiles (16x8 mma blocks never straddle two vars)
-    const int rows = (tv.card + 15) & ~15;
+    const int rows = big_pre ? (tv.card + 7) & ~7 : (tv.card + 15) & ~15;
     tv.dev_off = dev_row;
     tv.user_off = user_row;
     tv.ntile0 = dev_row / 8;
@@ -864,7 +889,9 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     g.hstride = off;
     std::vector<DpgGTile> tiles;
     std::vector<char> covered(g.NBT * (g.NBT + 1) / 2, 0);
-    for (int a = 0; a < g.ntest; a++)
+    // 16 x 8 blocks of the single-CTA kernel (large plans have none: their test vars may
+    // have an odd number of 8-row tiles)
+    for (int a = 0; a < g.ntest && !g.big; a++)
       for (int rp = 0; rp < g.test[a].ntiles; rp += 2) {
         const int I = g.test[a].ntile0 + rp;
         for (int b = 0; b <= a; b++)
@@ -886,15 +913,16 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     g.ngb = (int)tiles.size();
     g.ngt = g.NBT * (g.NBT + 1) / 2;
     std::vector<int> gz;  // lower tiles no block writes (uncoupled var pairs)
-    for (int u = 0; u < g.ngt; u++)
+    for (int u = 0; u < g.ngt && !g.big; u++)
       if (!covered[u]) gz.push_back(u);
     g.ngz = (int)gz.size();
     g.gzero = upload_i(P, gz);
     if (!g.big && (g.ngb + DPG_NWARPS - 1) / DPG_NWARPS > DPG_MAX_GT)
       return fail(DPG_ERR_UNSUPPORTED, "too many G blocks");
     void* p = nullptr;
-    if (cudaMalloc(&p, tiles.size() * sizeof(DpgGTile)) != cudaSuccess) return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
-    cudaMemcpy(p, tiles.data(), tiles.size() * sizeof(DpgGTile), cudaMemcpyHostToDevice);
+    if (cudaMalloc(&p, std::max<size_t>(1, tiles.size()) * sizeof(DpgGTile)) != cudaSuccess)
+      return fail(DPG_ERR_OUT_OF_MEMORY, "cudaMalloc");
+    if (!tiles.empty()) cudaMemcpy(p, tiles.data(), tiles.size() * sizeof(DpgGTile), cudaMemcpyHostToDevice);
     P->allocs.push_back(p);
     g.gtiles = (const DpgGTile*)p;
   }

@@ -218,8 +218,10 @@ static void geom_shape(const Topo& t, const double* xi, double* N, double* dN /*
 // optimized alpha table), and the Lagrange functions are built through the
 // orthonormal Proriol-Koornwinder-Dubiner (PKD) basis on the biunit triangle.
 // Basis_HDIV_TRI_In_FEM spans Raviart-Thomas RT_n (card n(n+2)); this file uses a
-// modal basis of the same space: (p, 0), (0, p) for p in P_{n-1}, then x h for
-// the homogeneous monomials h of degree n-1.  A test-space basis change leaves
+// modal basis of the same space: (p, 0), (0, p) for p in P_{n-1}, then x psi for
+// the orthonormal PKD polynomials psi of exact degree n-1 (their leading homogeneous
+// parts span the homogeneous polynomials of degree n-1; monomials there would make the
+// Gram matrix needlessly ill-conditioned at high degree).  A test-space basis change leaves
 // K, l and S unchanged (K = B^T G^-1 B is invariant under B -> T^T B, G -> T^T G T).
 // ----------------------------------------------------------------------------
 
@@ -385,9 +387,10 @@ static void tri_rt_eval(int n, const double* xi, double* val, double* div) {
       if (div) div[dof] = 2 * (c == 0 ? pr[k] : ps[k]);
     }
   for (int j = 0; j < n; j++, dof++) {
-    double h = std::pow(xi[0], n - 1 - j) * std::pow(xi[1], j);
-    if (val) { val[2 * dof] = xi[0] * h; val[2 * dof + 1] = xi[1] * h; }
-    if (div) div[dof] = (n + 1) * h;
+    double v, vr, vs;  // PKD polynomial of exact degree n-1; d/dxi = 2 d/dr
+    pkd_mode(n - 1 - j, j, 2 * xi[0] - 1, 2 * xi[1] - 1, v, vr, vs);
+    if (val) { val[2 * dof] = xi[0] * v; val[2 * dof + 1] = xi[1] * v; }
+    if (div) div[dof] = 2 * v + 2 * (xi[0] * vr + xi[1] * vs);
   }
 }
 

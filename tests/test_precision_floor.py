@@ -60,3 +60,24 @@ def test_fp64_gram_and_reduced_b_meet_the_bar(cells48, oracle_mod):
     P, o = cells48
     assert _worst_s_change(oracle_mod, P, o, 2.0 ** -53, "G") < 1e-10
     assert _worst_s_change(oracle_mod, P, o, 2.0 ** -40, "B") < 1e-10
+
+
+@pytest.mark.parametrize("p", [4, 6])
+def test_triangle_rt_basis_is_well_conditioned(oracle_mod, p):
+    """The triangle RT_n test basis (x psi with the PKD polynomials psi of exact degree n-1)
+    keeps the Stokes VGP triangle buckets' FP64 floor (relative change of K under 1-ulp noise
+    on G) at the level of the quad buckets: below 1e-11 on unit-size cells and below 1e-6 on
+    the finest cells of the uneven-cell workload (h = 1/256), where every factorisation
+    succeeds.  With x times monomials the floor was 1.4e-8 at h = 1 and the Gram matrix lost
+    positive definiteness at h = 1/256 for p = 6."""
+    from tests.test_gpu_parity import fp64_floor
+    b = fm.StokesVGPFormulation(2).bucket(abi.TOPO_TRI, p, 2)
+    P = oracle_mod.OraclePlan(b)
+    for base_n, bound in ((1, 1e-11), (256, 1e-6)):
+        nodes, par = mesh.forest_buckets(2000, seed=3, base_n=base_n, max_level=0)[(abi.TOPO_TRI, p)]
+        nodes, par = nodes[:2], par[:2]
+        co = mesh.uniform_coeff(2, P.info["n_slots"], P.info["n_points_total"], seed=1)
+        o = P.assemble(nodes, par, co, parts=True)
+        assert (o["info"] == 0).all()
+        floor = max(fp64_floor(oracle_mod, o["G"][c], o["B"][c], o["F"][c], o["K"][c], trials=2) for c in range(2))
+        assert floor < bound, (base_n, floor)
