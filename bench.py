@@ -57,7 +57,39 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the other configurations' timings")
     p.add_argument("--no-next", action="store_true",
                    help="skip the timings of the kernels after the assembly (recovery, energy, DLS, scatter)")
+    p.add_argument("--c3-bucket", default=None, metavar="quad_pK|tri_pK",
+                   help="small case for profiler captures: one Stokes VGP bucket (Delta p = 2) of the "
+                        "uneven-cell workload on --c3-cells jittered cells, one warm-up launch and one timed "
+                        "launch; prints one JSON line")
+    p.add_argument("--c3-cells", type=int, default=148)
     return p.parse_args()
+
+
+def run_c3_bucket(args):
+    """One bucket of the uneven-cell Stokes workload (small case for ncu captures)."""
+    import torch
+    from camellia2_b200 import abi, formulation as fm, lib, mesh
+    kind, p = args.c3_bucket.split("_p")
+    topo = abi.TOPO_QUAD if kind == "quad" else abi.TOPO_TRI
+    plan = lib.Plan(fm.StokesVGPFormulation(2).bucket(topo, int(p), 2))
+    n = int(np.ceil(np.sqrt(args.c3_cells)))
+    nodes, par = (mesh.quad_grid(n, n, 0.1, seed=1) if topo == abi.TOPO_QUAD else mesh.tri_grid(n, n, 0.1, seed=1))
+    nodes, par = nodes[:args.c3_cells], par[:args.c3_cells]
+    C = nodes.shape[0]
+    co = mesh.uniform_coeff(C, plan.info["n_slots"], plan.info["n_points_total"], seed=1)
+    dev = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()  # noqa: E731
+    dn, dp, dc = dev(nodes), dev(par), dev(co)
+    out = plan.alloc_outputs(C)
+    plan.assemble(dn, dp, dc, out=out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.assemble(dn, dp, dc, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    print(json.dumps({"c3_bucket": args.c3_bucket, "N": plan.info["N"], "M": plan.info["M"], "cells": C, "ms": ms,
+                      "cells_per_s": C / ms * 1e3, "info_nonzero_cells": int((out["info"] != 0).sum().item())}))
 
 
 def build_workload(n, seed):
@@ -408,6 +440,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.c3_bucket:
+        run_c3_bucket(args)
         return
     import torch
     import torch.distributed as dist
