@@ -27,7 +27,7 @@
 
 constexpr int ZT = 64;  // tile edge
 constexpr int ZL = 68;  // shared row stride, == 4 (mod 16) doubles: conflict-free DMMA fragments
-constexpr int ZK = 16;  // k-chunk of a formation tile (one m16n8k16 step)
+constexpr int ZK = 32;  // k-chunk of a formation tile (two m16n8k16 steps)
 constexpr int BIG_NOFAIL = 0x7fffffff;
 
 struct BigSm {
@@ -59,22 +59,28 @@ __device__ __forceinline__ BigSm big_views(const DpgPlanDev& P) {
   return S;
 }
 
-// acc (a 16 x 16 warp tile: rows wr.., columns wc..) += A B over one k16 step, operands stored
-// k-major: A[r][k] = fa[k][r], B[k][c] = fb[k][c].
+// acc (a 16 x 16 warp tile: rows wr.., columns wc..) += A B over one ZK chunk, operands stored
+// k-major: A[r][k] = fa[k][r], B[k][c] = fb[k][c].  The k16 steps alternate between acc and
+// acc2, so four independent DMMA chains are in flight.
 __device__ __forceinline__ void big_mma_kmajor(const double* fa, const double* fb, int wr, int wc, int g, int t,
-                                               double (&acc)[2][4]) {
-  double a[8];
+                                               double (&acc)[2][4], double (&acc2)[2][4]) {
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    a[2 * i] = fa[(t + 4 * i) * ZL + wr + g];
-    a[2 * i + 1] = fa[(t + 4 * i) * ZL + wr + g + 8];
-  }
+  for (int s16 = 0; s16 < ZK / 16; s16++) {
+    const double* fa_s = fa + s16 * 16 * ZL;
+    const double* fb_s = fb + s16 * 16 * ZL;
+    double a[8];
 #pragma unroll
-  for (int nb = 0; nb < 2; nb++) {
-    double b[4];
+    for (int i = 0; i < 4; i++) {
+      a[2 * i] = fa_s[(t + 4 * i) * ZL + wr + g];
+      a[2 * i + 1] = fa_s[(t + 4 * i) * ZL + wr + g + 8];
+    }
 #pragma unroll
-    for (int i = 0; i < 4; i++) b[i] = fb[(t + 4 * i) * ZL + wc + nb * 8 + g];
-    dmma16(acc[nb], a, b);
+    for (int nb = 0; nb < 2; nb++) {
+      double b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) b[i] = fb_s[(t + 4 * i) * ZL + wc + nb * 8 + g];
+      dmma16((s16 & 1) ? acc2[nb] : acc[nb], a, b);
+    }
   }
 }
 
@@ -210,29 +216,43 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
   }
   __syncthreads();
   const int nrel = relk[120], nk = relk[121];
-  double acc[2][4];
+  double acc[2][4], acc2[2][4];
 #pragma unroll
-  for (int nb = 0; nb < 2; nb++) acc[nb][0] = acc[nb][1] = acc[nb][2] = acc[nb][3] = 0.0;
+  for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+    for (int e = 0; e < 4; e++) acc[nb][e] = acc2[nb][e] = 0.0;
   // operands of k-chunk k0 (2 sides x ZK x 64 values) into buffer pair buf; chunk c + 1 is
-  // formed while the MMAs of chunk c run on the other pair, one barrier per chunk
+  // formed while the MMAs of chunk c run on the other pair, one barrier per chunk.  A thread's
+  // column is the same for every value it forms (NT is a multiple of 64), so its column records
+  // are read once per tile; all of a thread's values are computed before any is stored, so
+  // their loads overlap instead of waiting behind the shared-memory stores.
+  constexpr int NU = 2 * ZK * ZT / NT;
+  const int cc = tid & (ZT - 1);
+  int crec[2];
+#pragma unroll
+  for (int side = 0; side < 2; side++) {
+    const int i = (side ? c0 : r0) + cc;
+    crec[side] = (kind == 1 && side == 0) ? -1 : (i < P.Np ? S.col[i] : -1);
+  }
   auto operands = [&](int k0, int buf) {
     double* const fa = S.fa + buf * 2 * ZK * ZL;
-    double* const fb = fa + ZK * ZL;
-    for (int e = tid; e < 2 * ZK * ZT; e += NT) {
-      const int side = e >> 10, kl = (e >> 6) & (ZK - 1), c = e & (ZT - 1);
+    double vals[NU];
+#pragma unroll
+    for (int u = 0; u < NU; u++) {
+      const int e = tid + u * NT;
+      const int side = e / (ZK * ZT), kl = (e >> 6) & (ZK - 1);
       const int kk = k0 + kl;
       double val = 0.0;
       if (kk < nk) {
         if (kind == 0) {
-          const int ri = kk / P.QG, q = kk - ri * P.QG, r = rel[ri];
-          const int i = (side ? c0 : r0) + c;
-          const int rec = i < P.Np ? S.col[i] : -1;
+          const int rec = crec[side];
           if (rec >= 0) {
-            const int a = rec >> 16, il = rec & 0xffff;
-            const DpgTestVar& V = P.test[a];
+            const int ri = kk / P.QG, q = kk - ri * P.QG, r = rel[ri];
+            const int a = rec >> 16;
+            const int ld = P.test[a].ldA;
             const double* b = bh + ((size_t)(q * P.niprows + r) * P.ntest + a) * 4;
-            const double* f = P.frefG + (size_t)q * P.featstride + V.foff + il;
-            val = b[0] * __ldg(f) + b[1] * __ldg(f + V.ldA) + b[2] * __ldg(f + 2 * V.ldA) + b[3] * __ldg(f + 3 * V.ldA);
+            const double* f = P.frefG + (size_t)q * P.featstride + P.test[a].foff + (rec & 0xffff);
+            val = b[0] * __ldg(f) + b[1] * __ldg(f + ld) + b[2] * __ldg(f + 2 * ld) + b[3] * __ldg(f + 3 * ld);
             if (side == 0) val *= wq[q];
           }
         } else {
@@ -244,32 +264,41 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
           const DpgBTerm& Tm = P.bterm[Sg.term0 + be.y];
           const double* rq = Sg.rec + (size_t)q * Sg.rec_len;
           if (side == 0) {
-            const int j = r0 + c;
+            const int j = r0 + cc;
             if (j >= Tm.col0 && j < Tm.col0 + Tm.ncol) val = __ldg(rq + Sg.tvoff[be.y] + (j - Tm.col0));
           } else {
-            const int i = c0 + c;
-            const int rec = i < P.Np ? S.col[i] : -1;
+            const int rec = crec[1];
             if (rec >= 0 && (rec >> 16) == Tm.test_var) {
-              const DpgTestVar& V = P.test[Tm.test_var];
-              const double* f = rq + V.foff + (rec & 0xffff);
+              const int ld = P.test[Tm.test_var].ldA;
+              const double* f = rq + P.test[Tm.test_var].foff + (rec & 0xffff);
               const double* v4 = vt + (size_t)(be.z + q) * 4;
-              val = v4[0] * __ldg(f) + v4[1] * __ldg(f + V.ldA) + v4[2] * __ldg(f + 2 * V.ldA) +
-                    v4[3] * __ldg(f + 3 * V.ldA);
+              val = v4[0] * __ldg(f) + v4[1] * __ldg(f + ld) + v4[2] * __ldg(f + 2 * ld) + v4[3] * __ldg(f + 3 * ld);
             }
           }
         }
       }
-      (side ? fb : fa)[kl * ZL + c] = val;
+      vals[u] = val;
+    }
+#pragma unroll
+    for (int u = 0; u < NU; u++) {
+      const int e = tid + u * NT;
+      const int side = e / (ZK * ZT), kl = (e >> 6) & (ZK - 1);
+      fa[side * ZK * ZL + kl * ZL + cc] = vals[u];
     }
   };
   if (nk > 0) operands(0, 0);
   __syncthreads();
   for (int k0 = 0, c = 0; k0 < nk; k0 += ZK, c++) {
-    if (k0 + ZK < nk) operands(k0 + ZK, (c + 1) & 1);
+    // the products of chunk c are issued first, so they run while chunk c + 1's loads are in flight
     const double* fa = S.fa + (c & 1) * 2 * ZK * ZL;
-    big_mma_kmajor(fa, fa + ZK * ZL, wr, wc, g, t, acc);
+    big_mma_kmajor(fa, fa + ZK * ZL, wr, wc, g, t, acc, acc2);
+    if (k0 + ZK < nk) operands(k0 + ZK, (c + 1) & 1);
     __syncthreads();
   }
+#pragma unroll
+  for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+    for (int e = 0; e < 4; e++) acc[nb][e] += acc2[nb][e];
   const int ld = P.ldz;
   if (kind == 0) {
     if (diag) {
