@@ -366,7 +366,10 @@ __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, con
       S.Xi[r * ZL + c] = (r == c) ? 1.0 : 0.0;
     }
     __syncthreads();
-    // L_kk and L_kk^-1 together: column j of L, row j of the inverse, then the updates
+    // L_kk and L_kk^-1 together: column j of L (also copied to a contiguous vector, LI's first
+    // row, free until the panels), row j of the inverse, then the updates: 8 rows x 64 columns
+    // per pass of the block
+    double* const colj = S.LI;
     for (int j = 0; j < w; j++) {
       double piv = S.D[j * ZL + j];
       if (!(piv > 0.0)) {
@@ -375,17 +378,21 @@ __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, con
       }
       const double rinv = 1.0 / sqrt(piv);
       if (tid < ZT) {
-        if (tid > j && tid < w) S.D[tid * ZL + j] *= rinv;
+        if (tid > j && tid < w) {
+          const double v = S.D[tid * ZL + j] * rinv;
+          S.D[tid * ZL + j] = v;
+          colj[tid] = v;
+        }
         if (tid <= j) S.Xi[j * ZL + tid] *= rinv;
       }
       __syncthreads();
-      const int nr = w - j - 1;
-      for (int e = tid; e < nr * w; e += NT) {
-        const int rr = e / w, c = e - rr * w, r = j + 1 + rr;
-        const double lrj = S.D[r * ZL + j];
-        if (c <= j) S.Xi[r * ZL + c] -= lrj * S.Xi[j * ZL + c];
-        else if (c <= r) S.D[r * ZL + c] -= lrj * S.D[c * ZL + j];
-      }
+      const int c = tid & (ZT - 1);
+      if (c < w)
+        for (int r = j + 1 + (tid >> 6); r < w; r += NT / ZT) {
+          const double lrj = colj[r];
+          if (c <= j) S.Xi[r * ZL + c] -= lrj * S.Xi[j * ZL + c];
+          else if (c <= r) S.D[r * ZL + c] -= lrj * colj[c];
+        }
       __syncthreads();
     }
     // rows below the block: panel L_I = Z_I,k L_kk^-T (stored back), then Z_IJ -= L_I L_J^T
