@@ -234,6 +234,9 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
     const int i = (side ? c0 : r0) + cc;
     crec[side] = (kind == 1 && side == 0) ? -1 : (i < P.Np ? S.col[i] : -1);
   }
+  // kind 1: each thread's k index only grows (chunk by chunk, and with u inside a chunk), so the
+  // entry holding it is found by a forward cursor per side instead of a scan from the start
+  int ecur[2] = {0, 0};
   auto operands = [&](int k0, int buf) {
     double* const fa = S.fa + buf * 2 * ZK * ZL;
     double vals[NU];
@@ -256,8 +259,9 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
             if (side == 0) val *= wq[q];
           }
         } else {
-          int ei = 0;
+          int ei = ecur[side];
           while (ei + 1 < nrel && kk >= relk[ei + 1]) ei++;
+          ecur[side] = ei;
           const int4 be = P.be[rel[ei]];
           const int q = kk - relk[ei];
           const DpgSeg& Sg = P.seg[be.x];
