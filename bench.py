@@ -176,8 +176,9 @@ def c3_forest(torch, timeit, dev, total=100_000):
     """The uneven-cell Stokes VGP workload: ~100k cells (70 % quads, 30 % triangles, p uniform
     on 1..6, Delta p = 2, refinement level geometric on 0..4, jittered), twelve (topology, p)
     buckets in one CUDA graph: the single-CTA buckets in one persistent launch, the large ones
-    (quads p >= 3, triangles p >= 4) on the large-bucket kernel after it.  Per-bucket device
-    times come from single-bucket launches."""
+    (quads p >= 3, triangles p >= 4) on the large-bucket kernel after it.  Each single-CTA
+    bucket's Gram staging chunk is picked by dpg_plan_autotune on its own cells first.
+    Per-bucket device times come from single-bucket launches."""
     from camellia2_b200 import formulation as fm, lib, mesh
     form = fm.StokesVGPFormulation(2)
     items, keys, per = [], [], {}
@@ -190,10 +191,10 @@ def c3_forest(torch, timeit, dev, total=100_000):
     for key, (pl, dn, dp, dc, out) in zip(keys, items):
         C = dn.shape[0]
         N, M = pl.info["N"], pl.info["M"]
+        chunk = pl.autotune(dn, dp, dc)  # per-bucket Gram staging chunk, timed on these cells
         ms = timeit(lambda: pl.assemble(dn, dp, dc, out=out), reps=1)
-        big = (N + 15) // 16 * 16 > 192 or M > 120
         per[key] = {"cells": C, "N": N, "M": M, "ms": round(ms, 3), "cells_per_s": round(C / ms * 1e3),
-                    "kernel": "large-bucket" if big else "single-CTA"}
+                    "kernel": "single-CTA" if chunk else "large-bucket", "gram_chunk": chunk or None}
     g = lib.Graph(items)
     ms = timeit(g.launch, reps=2)
     bad = sum(int((it[4]["info"] != 0).sum().item()) for it in items)

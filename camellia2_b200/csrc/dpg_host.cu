@@ -476,6 +476,7 @@ struct HostPlan {
   size_t ws_bytes = 0;
   void* d_ws = nullptr;
   cudaStream_t streams[2] = {nullptr, nullptr};
+  bool adj_terms_ok = false;  // every coefficient use of the bucket is one the reverse mode covers
 };
 
 static double* upload(HostPlan* P, const std::vector<double>& v) {
@@ -584,6 +585,71 @@ static int big_layout(HostPlan* P) {
   g.bs_total = s;
   if ((size_t)s * 8 > 232448) return fail(DPG_ERR_UNSUPPORTED, "large-bucket kernel: shared memory exceeded");
   g.sm_total = s;
+  return DPG_OK;
+}
+
+// Shared-memory layout (doubles) of the single-CTA kernels for Gram chunks of chg points:
+// DPG_OK, -1 when it needs more shared memory than one CTA has, or a failure code.
+static int smem_layout(DpgPlanDev& g, int chg, bool adj_terms_ok) {
+  g.chg = chg;
+  auto al = [](int x) { return (x + 15) & ~15; };  // 128-byte aligned regions
+  int o = 0;
+  // Gram phase
+  g.g_fref0 = o; o += al(g.chg * g.featstride);
+  g.g_fref1 = o; o += al(g.chg * g.featstride);
+  g.g_h = o;
+  g.g_beta = o;  // per-point IP rows in reference slots; dead before the first h chunk
+  o += al(std::max(g.chg * g.hstride, g.QGpad * g.niprows * 4 * g.ntest));
+  g.g_geo = o; o += al(g.QGpad * 24);
+  g.g_D = o; o += al(g.QGpad * g.npairs * 16);
+  int gphase = o;
+  // factor
+  o = 0;
+  g.sm_gt = o; o += al(g.ngt * 64);
+  g.sm_linv = o; o += al(g.NBT * 64);
+  g.sm_scale = o; o += al(g.Np);
+  int fphase = o;
+  // B phase (runs first; whole body available)
+  o = 0;
+  g.b_rec0 = o; o += al(g.max_chunk * g.max_rec);
+  g.b_rec1 = o; o += al(g.max_chunk * g.max_rec);
+  g.b_u = o; o += al(g.max_chunk * g.max_ustride);
+  g.b_geo = o; o += al(g.nbpts * 24);
+  g.b_fac = o; o += al(g.nse * g.QS);
+  int bphase = o;
+  g.sm_w = 0;
+  int wsz = g.MBT * g.NBT * 64;
+  g.sm_k = 0;
+  int ksz = g.MBT * (g.MBT + 1) / 2 * 64;
+  if (g.sm_linv < ksz || g.sm_linv + g.MBT * 64 > g.sm_linv + al(g.NBT * 64))
+    return fail(DPG_ERR_UNSUPPORTED, "trial tiles outnumber test tiles: condensation workspace overlaps K");
+  int body = std::max(std::max(gphase, bphase), std::max(std::max(wsz, ksz), fphase));
+  // reverse mode: S_A, then the pull-back staging (both reuse the body after the factor)
+  {
+    const int Mx = g.MBT * 8;
+    g.a_ldS = ((Mx + 15) & ~15) + 4;  // == 4 mod 16: conflict-free B-fragments
+    g.a_sa = 0;
+    const int sa_end = Mx * g.a_ldS;
+    int fsl = g.featstride;
+    if (g.seg[0].nterm > 0) fsl = std::max(fsl, g.seg[0].rec_len);
+    int q = 0;
+    g.a_fs = q; q += al(DPG_CHA_HOST * fsl);
+    g.a_ldx = 2 * Mx;
+    g.a_xpf = q; q += al(DPG_CHA_HOST * g.ntest * 4 * g.a_ldx);
+    g.a_geo = q; q += al(std::max(DPG_CHA_HOST, g.ns * g.QS) * 24);
+    g.a_beta = q; q += al(DPG_CHA_HOST * g.niprows * 4 * g.ntest);
+    g.a_cbar = q; q += al(std::max(1, g.nslots * g.Ptot));
+    g.adj_ok = adj_terms_ok && std::max(sa_end, q) <= body && g.QB > 0;
+  }
+  g.sm_coef = al(body);
+  g.sm_tiles = g.sm_coef + al(std::max(1, g.nslots * g.Ptot));
+  g.sm_nodes = g.sm_tiles + al((g.ngb * (int)sizeof(DpgGTile) + 7) / 8);
+  g.sm_invd = g.sm_nodes + 192;
+  g.sm_total = g.sm_invd + al(std::max(g.Np, g.Mp));
+  if ((size_t)g.sm_total * 8 > 232448) {
+    return -1;
+  }
+  g.scratch_per_cta = (size_t)g.MBT * g.NBT * 64;
   return DPG_OK;
 }
 
@@ -1269,68 +1335,13 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
     if (rc != DPG_OK) return rc;
   }
   // ---- shared memory layout (doubles) ----------------------------------------
-  for (g.chg = DPG_CHG; !g.big; g.chg /= 2) {
-    auto al = [](int x) { return (x + 15) & ~15; };  // 128-byte aligned regions
-    int o = 0;
-    // Gram phase
-    g.g_fref0 = o; o += al(g.chg * g.featstride);
-    g.g_fref1 = o; o += al(g.chg * g.featstride);
-    g.g_h = o;
-    g.g_beta = o;  // per-point IP rows in reference slots; dead before the first h chunk
-    o += al(std::max(g.chg * g.hstride, g.QGpad * g.niprows * 4 * g.ntest));
-    g.g_geo = o; o += al(g.QGpad * 24);
-    g.g_D = o; o += al(g.QGpad * g.npairs * 16);
-    int gphase = o;
-    // factor
-    o = 0;
-    g.sm_gt = o; o += al(g.ngt * 64);
-    g.sm_linv = o; o += al(g.NBT * 64);
-    g.sm_scale = o; o += al(g.Np);
-    int fphase = o;
-    // B phase (runs first; whole body available)
-    o = 0;
-    g.b_rec0 = o; o += al(g.max_chunk * g.max_rec);
-    g.b_rec1 = o; o += al(g.max_chunk * g.max_rec);
-    g.b_u = o; o += al(g.max_chunk * g.max_ustride);
-    g.b_geo = o; o += al(g.nbpts * 24);
-    g.b_fac = o; o += al(g.nse * g.QS);
-    int bphase = o;
-    g.sm_w = 0;
-    int wsz = g.MBT * g.NBT * 64;
-    g.sm_k = 0;
-    int ksz = g.MBT * (g.MBT + 1) / 2 * 64;
-    if (g.sm_linv < ksz || g.sm_linv + g.MBT * 64 > g.sm_linv + al(g.NBT * 64))
-      return fail(DPG_ERR_UNSUPPORTED, "trial tiles outnumber test tiles: condensation workspace overlaps K");
-    int body = std::max(std::max(gphase, bphase), std::max(std::max(wsz, ksz), fphase));
-    // reverse mode: S_A, then the pull-back staging (both reuse the body after the factor)
-    {
-      const int Mx = g.MBT * 8;
-      g.a_ldS = ((Mx + 15) & ~15) + 4;  // == 4 mod 16: conflict-free B-fragments
-      g.a_sa = 0;
-      const int sa_end = Mx * g.a_ldS;
-      int fsl = g.featstride;
-      if (g.seg[0].nterm > 0) fsl = std::max(fsl, g.seg[0].rec_len);
-      int q = 0;
-      g.a_fs = q; q += al(DPG_CHA_HOST * fsl);
-      g.a_ldx = 2 * Mx;
-      g.a_xpf = q; q += al(DPG_CHA_HOST * g.ntest * 4 * g.a_ldx);
-      g.a_geo = q; q += al(std::max(DPG_CHA_HOST, g.ns * g.QS) * 24);
-      g.a_beta = q; q += al(DPG_CHA_HOST * g.niprows * 4 * g.ntest);
-      g.a_cbar = q; q += al(std::max(1, g.nslots * g.Ptot));
-      g.adj_ok = adj_terms_ok && std::max(sa_end, q) <= body && g.QB > 0;
-    }
-    g.sm_coef = al(body);
-    g.sm_tiles = g.sm_coef + al(std::max(1, g.nslots * g.Ptot));
-    g.sm_nodes = g.sm_tiles + al((g.ngb * (int)sizeof(DpgGTile) + 7) / 8);
-    g.sm_invd = g.sm_nodes + 192;
-    g.sm_total = g.sm_invd + al(std::max(g.Np, g.Mp));
-    if ((size_t)g.sm_total * 8 > 232448) {
-      if (g.chg > DPG_CHG / 2) continue;  // retry with half-size Gram chunks
-      return fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
-    }
-    g.scratch_per_cta = (size_t)g.MBT * g.NBT * 64;
-    break;
+  if (!g.big) {
+    int rc = smem_layout(g, DPG_CHG, adj_terms_ok);
+    if (rc == -1) rc = smem_layout(g, DPG_CHG / 2, adj_terms_ok);  // half-size Gram chunks
+    if (rc == -1) return fail(DPG_ERR_UNSUPPORTED, "bucket needs more shared memory than one CTA has");
+    if (rc != DPG_OK) return rc;
   }
+  P->adj_terms_ok = adj_terms_ok;
   // info
   dpg_plan_info& I = P->info;
   I.N = g.N; I.M = g.M; I.n_field = g.nf; I.n_trace = g.nt;
@@ -1540,6 +1551,62 @@ int dpg_assemble(dpg_plan* p, int C, const double* nodes, const int8_t* parity, 
   L.s = (flags & DPG_FLAG_NO_CONDENSE) ? nullptr : s;
   L.info = info;
   return dpg_launch_assemble(&p->hp.dev, p->hp.d_dev, &L, (cudaStream_t)stream);
+}
+
+int dpg_plan_autotune(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff, void* stream,
+                      int* chosen) {
+  if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
+  if (!chosen) return fail(DPG_ERR_INVALID_ARGUMENT, "null output");
+  *chosen = 0;
+  if (p->hp.dev.big) return DPG_OK;  // the large-bucket kernel has one configuration
+  if (C <= 0 || !nodes || !parity) return fail(DPG_ERR_INVALID_ARGUMENT, "cells, nodes and parity are required");
+  if (p->hp.dev.nslots > 0 && !coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
+  cudaStream_t st = (cudaStream_t)stream;
+  const DpgPlanDev& g0 = p->hp.dev;
+  const size_t nK = (size_t)C * g0.M * g0.M, nl = (size_t)C * g0.M, nS = (size_t)C * g0.nt * g0.nt, ns = (size_t)C * g0.nt;
+  void* out = nullptr;
+  if (cudaMallocAsync(&out, (nK + nl + nS + ns) * sizeof(double) + (size_t)C * 4, st) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DPG_ERR_OUT_OF_MEMORY, "autotune outputs");
+  }
+  DpgLaunch L;
+  std::memset(&L, 0, sizeof(L));
+  L.C = C; L.nodes = nodes; L.parity = parity; L.coeff = coeff;
+  L.K = (double*)out; L.l = L.K + nK; L.S = L.l + nl; L.s = L.S + nS; L.info = (int32_t*)(L.s + ns);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = -1.0f;
+  DpgPlanDev best_plan = g0;
+  int rc = DPG_OK;
+  for (int chg = DPG_CHG; chg >= DPG_CHG / 2 && rc == DPG_OK; chg /= 2) {
+    DpgPlanDev cand = g0;
+    if (smem_layout(cand, chg, p->hp.adj_terms_ok) != DPG_OK) continue;
+    if ((rc = dpg_configure_kernels(&cand)) != DPG_OK) break;
+    if ((rc = dpg_launch_assemble(&cand, nullptr, &L, st)) != DPG_OK) break;  // warm-up
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 2 && rc == DPG_OK; r++) rc = dpg_launch_assemble(&cand, nullptr, &L, st);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(DPG_ERR_CUDA, "autotune timing");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rc == DPG_OK && (best < 0.0f || ms < best)) {
+      best = ms;
+      best_plan = cand;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(out, st);
+  if (rc != DPG_OK) return rc;
+  if (best < 0.0f) return fail(DPG_ERR_UNSUPPORTED, "no Gram chunk size fits this bucket");
+  p->hp.dev = best_plan;
+  if (cudaMemcpy(p->hp.d_dev, &p->hp.dev, sizeof(DpgPlanDev), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(DPG_ERR_CUDA, "plan upload");
+  rc = dpg_configure_kernels(&p->hp.dev);
+  if (rc != DPG_OK) return rc;
+  *chosen = p->hp.dev.chg;
+  return DPG_OK;
 }
 
 int dpg_assemble_noalloc(dpg_plan* p, int C, const double* nodes, const int8_t* parity, const double* coeff,

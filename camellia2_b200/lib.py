@@ -46,6 +46,7 @@ def load():
     L.dpg_plan_create.argtypes = [vp, ct.POINTER(vp)]
     L.dpg_plan_destroy.argtypes = [vp]
     L.dpg_plan_query.argtypes = [vp, vp]
+    L.dpg_plan_autotune.argtypes = [vp, i, vp, vp, vp, vp, ct.POINTER(i)]
     L.dpg_assemble.argtypes = [vp, i] + [vp] * 8 + [vp, i]
     L.dpg_assemble_host.argtypes = [vp, i] + [vp] * 8 + [i]
     L.dpg_assemble_parts.argtypes = [vp, i] + [vp] * 6 + [vp]
@@ -138,6 +139,14 @@ class Plan:
     def localStiffnessMatrixAndRHS(self, nodes, parity, coeff=None):
         o = self.assemble(nodes, parity, coeff)
         return o["K"], o["l"]
+
+    def autotune(self, nodes, parity, coeff=None, stream=None):
+        """dpg_plan_autotune: time the Gram staging chunk sizes that fit on these cells (device
+        tensors) and keep the faster; returns the chosen chunk (0 for a large-bucket plan)."""
+        chosen = ct.c_int(0)
+        _check(load().dpg_plan_autotune(self.h, nodes.shape[0], _ptr(nodes), _ptr(parity), _ptr(coeff),
+                                        _stream_ptr(stream), ct.byref(chosen)))
+        return chosen.value
 
     def parts(self, nodes, parity, coeff=None, stream=None):
         import torch

@@ -40,6 +40,7 @@
  *                             TRHS::integrateAgainstStandardBasis (src/Problem/RHS.cpp:68-82)
  *   dpg_factored_cholesky_solve  TBF::factoredCholeskySolve (src/ScratchPad/BF.cpp:924-1018)
  *   dpg_assemble_adjoint      no counterpart in the reference (new capability)
+ *   dpg_plan_autotune         no counterpart in the reference (GPU launch configuration)
  *   dpg_assemble_dls          TBF::localStiffnessMatrixAndRHS_DLS (src/ScratchPad/BF.cpp:1169-1306)
  *   dpg_scatter_global        GDAMinimumRule::interpretLocalData + global insertion
  *                             (src/Mesh/GDAMinimumRule.cpp:714-800, src/Solution/Solution.cpp:1263-1293)
@@ -195,6 +196,18 @@ typedef struct dpg_plan dpg_plan;
 int dpg_plan_create(const dpg_bucket_desc* desc, dpg_plan** plan);
 int dpg_plan_destroy(dpg_plan* plan);
 int dpg_plan_query(const dpg_plan* plan, dpg_plan_info* info);
+
+/* Per-bucket autotuner (no counterpart in the reference: Camellia has no GPU
+ * launch shapes to choose).  Times dpg_assemble on the C given cells (DEVICE
+ * pointers as for dpg_assemble) with each Gram staging chunk that fits the
+ * bucket's shared memory (8 and 4 quadrature points per chunk: the chunk sets
+ * the shared-memory layout and the kernel instance), keeps the faster for all
+ * later calls on this plan and returns its chunk size in *chosen (0 for a
+ * large-bucket plan, which has a single configuration).  Results of the two
+ * configurations agree to rounding (the Gram sums are ordered differently).
+ * Allocates its timing outputs from the stream-ordered pool. */
+int dpg_plan_autotune(dpg_plan* plan, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                      void* stream, int* chosen);
 
 /* Assemble C cells; all pointers are DEVICE pointers.
  *   nodes  (C, n_vertices, space_dim)   physical vertex coordinates
