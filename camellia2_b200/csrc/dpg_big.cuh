@@ -513,6 +513,36 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
       for (int J = 0; J < I; J++) big_form_tile(P, L, 0, I * ZT, J * ZT, false, Z, S, wq, bh, vt);
     for (int J = 0; J < nbm; J++)
       for (int I = 0; I < nbg; I++) big_form_tile(P, L, 1, J * ZT, I * ZT, false, Z, S, wq, bh, vt);
+    if (L.parts) {
+      // G (N, N), B (M, N) and F (N) in user numbering: Z unscaled (dpg_assemble_parts)
+      __syncthreads();
+      const int N = P.N;
+      auto dev_test = [&](int u) {
+        int dv = 0;
+        for (int a = 0; a < P.ntest; a++)
+          if (u >= P.test[a].user_off && u < P.test[a].user_off + P.test[a].card) dv = P.test[a].dev_off + u - P.test[a].user_off;
+        return dv;
+      };
+      if (L.G)
+        for (size_t e = tid; e < (size_t)N * N; e += NT) {
+          const int ur = (int)(e / N), uc = (int)(e - (size_t)ur * N);
+          const int dr = dev_test(ur), dc = dev_test(uc);
+          L.G[(size_t)cell * N * N + e] = Z[(size_t)max(dr, dc) * ld + min(dr, dc)] / (S.sc[dr] * S.sc[dc]);
+        }
+      if (L.B)
+        for (size_t e = tid; e < (size_t)M * N; e += NT) {
+          const int ut = (int)(e / N), us = (int)(e - (size_t)ut * N);
+          const int ds = dev_test(us);
+          L.B[(size_t)cell * M * N + e] = Z[(size_t)(Np + __ldg(P.u2d_trial + ut)) * ld + ds] / S.sc[ds];
+        }
+      if (L.F)
+        for (int us = tid; us < N; us += NT) {
+          const int ds = dev_test(us);
+          L.F[(size_t)cell * N + us] = Z[(size_t)(Np + P.fcol) * ld + ds] / S.sc[ds];
+        }
+      __syncthreads();
+      continue;
+    }
     big_cholesky(P, Z, 0, Np, S, &S.ints[0]);
     // trailing block = -[K_ext]: K, l out, then negate (padded field columns get a unit pivot)
     const double* T = Z + (size_t)Np * ld + Np;

@@ -1252,7 +1252,7 @@ static int configure_big(const DpgPlanDev* plan) {
 
 // Large buckets: one CTA per SM, each with its own workspace (Z and the per-point factors).
 static int launch_big(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
-  if (Lin->parts || Lin->solve_only)
+  if (Lin->solve_only)
     return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans support the assembly entry points only");
   const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
   DpgLaunch L = *Lin;

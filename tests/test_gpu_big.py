@@ -97,9 +97,28 @@ def test_big_bucket_rejects_unsupported_entry_points():
     form, bucket, nodes, par = stokes2d(3, 2, 1, 1, 0.1)
     plan = dlib.Plan(bucket)
     co = coeffs_for(bucket, plan.info, 1)
+    M = plan.info["M"]
     with pytest.raises(dlib.DpgError) as ei:
-        plan.parts(_dev(nodes), _dev(par), _dev(co))
+        plan.adjoint(_dev(nodes), _dev(par), _dev(co), _dev(np.eye(M)[None]), _dev(np.ones((1, M))))
     assert ei.value.code == 2
+
+
+@pytest.mark.parametrize("name", ["stokes2d_k6_dk2", "stokes_tri_k4_dk2", "poisson3d_k3_dk1"])
+def test_big_bucket_parts_match_oracle(name, oracle_mod):
+    """dpg_assemble_parts on large buckets: G, B, F to 1e-13 relative Frobenius per cell."""
+    form, bucket, nodes, par = CASES[name]()
+    P = oracle_mod.OraclePlan(bucket)
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, P.info, C)
+    ref = P.assemble(nodes, par, co, parts=True)
+    plan = dlib.Plan(bucket)
+    G, B, F = plan.parts(_dev(nodes), _dev(par), None if co is None else _dev(co))
+    torch.cuda.synchronize()
+    G, B, F = G.cpu().numpy(), B.cpu().numpy(), F.cpu().numpy()
+    for c in range(C):
+        assert rel_fro(G[c], ref["G"][c]) < 1e-13
+        assert rel_fro(B[c], ref["B"][c]) < 1e-13
+        assert rel_fro(F[c], ref["F"][c]) < 1e-13
 
 
 def _mixed_buckets():
