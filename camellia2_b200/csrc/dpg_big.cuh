@@ -544,6 +544,26 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
       continue;
     }
     big_cholesky(P, Z, 0, Np, S, &S.ints[0]);
+    if (L.energy) {
+      // energy error (dpg_energy_error): the rows below the test block now hold W = L^-1 E, so
+      // e^2 = || L^-1 F - L^-1 B^T x ||^2 is a sum over the test rows, with no cancellation
+      const double* x = L.xsol + (size_t)cell * M;
+      double part = 0.0;
+      for (int k = tid; k < Np; k += NT) {
+        double r = Z[(size_t)(Np + P.fcol) * ld + k];
+        for (int ut = 0; ut < M; ut++) r -= Z[(size_t)(Np + __ldg(P.u2d_trial + ut)) * ld + k] * x[ut];
+        part += r * r;
+      }
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      double* red = S.LI;  // free after the factorisation
+      if ((tid & 31) == 0) red[tid >> 5] = part;
+      __syncthreads();
+      if (tid == 0) {
+        double e2 = 0.0;
+        for (int w = 0; w < NT / 32; w++) e2 += red[w];
+        L.energy[cell] = sqrt(e2);
+      }
+    } else {
     // trailing block = -[K_ext]: K, l out, then negate (padded field columns get a unit pivot)
     const double* T = Z + (size_t)Np * ld + Np;
     if (L.K)
@@ -573,6 +593,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
         }
       if (L.s)
         for (int u = tid; u < nt; u += NT) L.s[(size_t)cell * nt + u] = T[(size_t)P.fcol * ld + __ldg(P.u2d_trial + nf + u)];
+    }
     }
     __syncthreads();
     if (tid == 0 && L.info) {

@@ -156,3 +156,23 @@ def test_multi_and_graph_with_large_buckets():
         for k in ("K", "l", "S", "s", "info"):
             assert torch.equal(out[k], ref[k]), k
     g.close()
+
+
+@pytest.mark.parametrize("name", ["stokes2d_k3_dk2", "stokes2d_k6_dk2", "stokes_tri_k4_dk2"])
+def test_big_bucket_energy_error_matches_oracle(name, oracle_mod):
+    """dpg_energy_error on large buckets: sqrt(r^T G^-1 r), r = F - B x, for random local trial
+    coefficients x, against a dense solve with the oracle's G, B, F (1e-10 relative)."""
+    form, bucket, nodes, par = CASES[name]()
+    plan = dlib.Plan(bucket)
+    C, M = nodes.shape[0], plan.info["M"]
+    co = coeffs_for(bucket, plan.info, C)
+    x = np.random.default_rng(4).normal(size=(C, M))
+    e, info = plan.energy_error(_dev(nodes), _dev(par), _dev(co), _dev(x))
+    torch.cuda.synchronize()
+    assert int(info.abs().max()) == 0
+    e = e.cpu().numpy()
+    G, B, F = oracle_mod.OraclePlan(bucket).parts(nodes, par, co)
+    for c in range(C):
+        r = F[c] - B[c].T @ x[c]
+        ref = np.sqrt(r @ np.linalg.solve(G[c], r))
+        assert abs(e[c] - ref) <= 1e-10 * ref, (c, e[c], ref)
