@@ -40,6 +40,15 @@
 //                    (Epetra_SerialDenseSolver: optional DGEEQU equilibration,
 //                    LU with partial pivoting)
 //
+// Precision.  The same source builds twice (oracle/build.sh): liboracle.so with
+// `real` = double, the FP64 oracle the GPU path is compared with, and
+// liboracle_xp.so with `real` = __float128 (113-bit significand, libquadmath), the
+// extended-precision truth that measures how far each FP64 code is from the exact
+// result of the same double inputs (nodes, coefficients).  Everything between the
+// inputs and the outputs -- cubature points and weights, basis tables, geometry,
+// products, factorisations -- runs in `real`; the C interface below converts at the
+// boundary.
+//
 // Third-party arithmetic restated here (not present under the reference tree):
 // Intrepid (Trilinos, version unpinned by the reference: "a recent version",
 // trilinos-fixes targets 12.6.4) bases, cubature and FunctionSpaceTools; LAPACK
@@ -55,7 +64,40 @@
 #include <vector>
 #include <string>
 
-namespace orc {
+#ifdef ORC_QUAD
+#include <quadmath.h>
+#define ORC_NS orc_xp
+#else
+#define ORC_NS orc
+#endif
+
+namespace ORC_NS {
+#ifdef ORC_QUAD
+typedef __float128 real;
+static inline real r_sqrt(real x) { return sqrtq(x); }
+static inline real r_fabs(real x) { return fabsq(x); }
+static inline real r_cos(real x) { return cosq(x); }
+static inline real r_sin(real x) { return sinq(x); }
+static inline real r_pow(real a, real b) { return powq(a, b); }
+static inline real r_tgamma(real x) { return tgammaq(x); }
+static inline bool r_isnan(real x) { return isnanq(x); }
+static const real R_PI = M_PIq;
+static const real R_NEWTON_TOL = 1e-32;
+#else
+typedef double real;
+static inline real r_sqrt(real x) { return std::sqrt(x); }
+static inline real r_fabs(real x) { return std::fabs(x); }
+static inline real r_cos(real x) { return std::cos(x); }
+static inline real r_sin(real x) { return std::sin(x); }
+static inline real r_pow(real a, real b) { return std::pow(a, b); }
+static inline real r_tgamma(real x) { return std::tgamma(x); }
+static inline bool r_isnan(real x) { return std::isnan(x); }
+static const real R_PI = M_PI;
+static const real R_NEWTON_TOL = 1e-16;
+#endif
+}  // namespace ORC_NS
+
+namespace ORC_NS {
 
 using std::vector;
 
@@ -64,29 +106,29 @@ using std::vector;
 // ----------------------------------------------------------------------------
 
 // Legendre P_n and derivative at x by the three-term recurrence.
-static void legendre(int n, double x, double& p, double& dp) {
-  double p0 = 1.0, p1 = x;
+static void legendre(int n, real x, real& p, real& dp) {
+  real p0 = 1.0, p1 = x;
   if (n == 0) { p = 1.0; dp = 0.0; return; }
   for (int k = 2; k <= n; k++) {
-    double pk = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+    real pk = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
     p0 = p1; p1 = pk;
   }
   p = p1;
-  dp = (std::fabs(1.0 - x * x) < 1e-300) ? 0.0 : n * (p0 - x * p1) / (1.0 - x * x);
+  dp = (r_fabs(1.0 - x * x) < 1e-300) ? 0.0 : n * (p0 - x * p1) / (1.0 - x * x);
 }
 
 // Gauss-Legendre n-point rule on [-1,1], ascending nodes.
-void gauss_legendre(int n, double* x, double* w) {
+void gauss_legendre(int n, real* x, real* w) {
   for (int i = 0; i < n; i++) {
-    double xi = -std::cos(M_PI * (i + 0.75) / (n + 0.5));
+    real xi = -r_cos(R_PI * (i + 0.75) / (n + 0.5));
     for (int it = 0; it < 100; it++) {
-      double p, dp;
+      real p, dp;
       legendre(n, xi, p, dp);
-      double dx = p / dp;
+      real dx = p / dp;
       xi -= dx;
-      if (std::fabs(dx) < 1e-16) break;
+      if (r_fabs(dx) < R_NEWTON_TOL) break;
     }
-    double p, dp;
+    real p, dp;
     legendre(n, xi, p, dp);
     x[i] = xi;
     w[i] = 2.0 / ((1.0 - xi * xi) * dp * dp);
@@ -94,25 +136,25 @@ void gauss_legendre(int n, double* x, double* w) {
 }
 
 // Gauss-Lobatto nodes (p+1 of them) for degree p >= 1: +-1 and the roots of P'_p.
-void gauss_lobatto(int p, double* x) {
+void gauss_lobatto(int p, real* x) {
   x[0] = -1.0;
   x[p] = 1.0;
   for (int i = 1; i < p; i++) {
-    double xi = -std::cos(M_PI * i / p);
+    real xi = -r_cos(R_PI * i / p);
     for (int it = 0; it < 100; it++) {
-      double P, dP;
+      real P, dP;
       legendre(p, xi, P, dP);
-      double d2P = (2.0 * xi * dP - p * (p + 1.0) * P) / (1.0 - xi * xi);
-      double dx = dP / d2P;
+      real d2P = (2.0 * xi * dP - p * (p + 1.0) * P) / (1.0 - xi * xi);
+      real dx = dP / d2P;
       xi -= dx;
-      if (std::fabs(dx) < 1e-16) break;
+      if (r_fabs(dx) < R_NEWTON_TOL) break;
     }
     x[i] = xi;
   }
 }
 
 // Lagrange polynomial i on `nodes` (size m) and its derivative at x.
-static void lagrange(const vector<double>& nodes, int i, double x, double& v, double& dv) {
+static void lagrange(const vector<real>& nodes, int i, real x, real& v, real& dv) {
   int m = (int)nodes.size();
   v = 1.0;
   for (int j = 0; j < m; j++)
@@ -120,7 +162,7 @@ static void lagrange(const vector<double>& nodes, int i, double x, double& v, do
   dv = 0.0;
   for (int k = 0; k < m; k++) {
     if (k == i) continue;
-    double t = 1.0 / (nodes[i] - nodes[k]);
+    real t = 1.0 / (nodes[i] - nodes[k]);
     for (int j = 0; j < m; j++)
       if (j != i && j != k) t *= (x - nodes[j]) / (nodes[i] - nodes[j]);
     dv += t;
@@ -130,18 +172,18 @@ static void lagrange(const vector<double>& nodes, int i, double x, double& v, do
 // 1D nodal family: "closed" (Gauss-Lobatto, degree n, n+1 nodes) or "open"
 // (Gauss-Legendre, degree n, n+1 nodes).  Degree 0 closed = constant.
 struct Nodal1D {
-  vector<double> nodes;
+  vector<real> nodes;
   void closed(int n) {
     nodes.assign(n + 1, 0.0);
     if (n >= 1) gauss_lobatto(n, nodes.data());
   }
   void open(int n) {
     nodes.assign(n + 1, 0.0);
-    vector<double> w(n + 1);
+    vector<real> w(n + 1);
     gauss_legendre(n + 1, nodes.data(), w.data());
   }
   int size() const { return (int)nodes.size(); }
-  void eval(int i, double x, double& v, double& dv) const {
+  void eval(int i, real x, real& v, real& dv) const {
     if (nodes.size() == 1) { v = 1.0; dv = 0.0; return; }
     lagrange(nodes, i, x, v, dv);
   }
@@ -153,7 +195,7 @@ struct Nodal1D {
 
 struct Topo {
   int key = 0, d = 0, nv = 0, nsides = 0, side_nv = 0;
-  double v[8][3] = {};
+  real v[8][3] = {};
   int sv[6][4] = {};
 };
 
@@ -162,12 +204,12 @@ static Topo make_topo(int key) {
   t.key = key;
   if (key == DPG_TOPO_QUAD) {
     t.d = 2; t.nv = 4; t.nsides = 4; t.side_nv = 2;
-    double v[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+    real v[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
     for (int i = 0; i < 4; i++) { t.v[i][0] = v[i][0]; t.v[i][1] = v[i][1]; }
     for (int s = 0; s < 4; s++) { t.sv[s][0] = s; t.sv[s][1] = (s + 1) % 4; }
   } else if (key == DPG_TOPO_HEX) {
     t.d = 3; t.nv = 8; t.nsides = 6; t.side_nv = 4;
-    double v[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+    real v[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
                       {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
     for (int i = 0; i < 8; i++) for (int k = 0; k < 3; k++) t.v[i][k] = v[i][k];
     // shards Hexahedron<8> face node lists
@@ -175,7 +217,7 @@ static Topo make_topo(int key) {
     for (int s = 0; s < 6; s++) for (int k = 0; k < 4; k++) t.sv[s][k] = f[s][k];
   } else if (key == DPG_TOPO_TRI) {
     t.d = 2; t.nv = 3; t.nsides = 3; t.side_nv = 2;
-    double v[3][2] = {{0, 0}, {1, 0}, {0, 1}};
+    real v[3][2] = {{0, 0}, {1, 0}, {0, 1}};
     for (int i = 0; i < 3; i++) { t.v[i][0] = v[i][0]; t.v[i][1] = v[i][1]; }
     for (int s = 0; s < 3; s++) { t.sv[s][0] = s; t.sv[s][1] = (s + 1) % 3; }
   }
@@ -183,23 +225,23 @@ static Topo make_topo(int key) {
 }
 
 // Vertex shape functions of the geometric map (HGRAD C1, vertex ordered).
-static void geom_shape(const Topo& t, const double* xi, double* N, double* dN /*nv x d*/) {
+static void geom_shape(const Topo& t, const real* xi, real* N, real* dN /*nv x d*/) {
   if (t.key == DPG_TOPO_TRI) {
     N[0] = 1 - xi[0] - xi[1]; N[1] = xi[0]; N[2] = xi[1];
     dN[0] = -1; dN[1] = -1; dN[2] = 1; dN[3] = 0; dN[4] = 0; dN[5] = 1;
     return;
   }
   for (int a = 0; a < t.nv; a++) {
-    double f[3], df[3];
+    real f[3], df[3];
     for (int k = 0; k < t.d; k++) {
       f[k] = 0.5 * (1.0 + xi[k] * t.v[a][k]);
       df[k] = 0.5 * t.v[a][k];
     }
-    double prod = 1.0;
+    real prod = 1.0;
     for (int k = 0; k < t.d; k++) prod *= f[k];
     N[a] = prod;
     for (int k = 0; k < t.d; k++) {
-      double g = df[k];
+      real g = df[k];
       for (int m = 0; m < t.d; m++) if (m != k) g *= f[m];
       dN[a * t.d + k] = g;
     }
@@ -226,81 +268,81 @@ static void geom_shape(const Topo& t, const double* xi, double* N, double* dN /*
 // ----------------------------------------------------------------------------
 
 // Orthonormal Jacobi polynomial P_n^{(a,b)}(x) on [-1,1] (weight (1-x)^a (1+x)^b).
-static double jacobi(double x, double a, double b, int n) {
-  double g0 = std::pow(2.0, a + b + 1) / (a + b + 1) * std::tgamma(a + 1) * std::tgamma(b + 1) / std::tgamma(a + b + 1);
-  double p0 = 1.0 / std::sqrt(g0);
+static real jacobi(real x, real a, real b, int n) {
+  real g0 = r_pow(2.0, a + b + 1) / (a + b + 1) * r_tgamma(a + 1) * r_tgamma(b + 1) / r_tgamma(a + b + 1);
+  real p0 = 1.0 / r_sqrt(g0);
   if (n == 0) return p0;
-  double g1 = (a + 1) * (b + 1) / (a + b + 3) * g0;
-  double p1 = ((a + b + 2) * x / 2 + (a - b) / 2) / std::sqrt(g1);
+  real g1 = (a + 1) * (b + 1) / (a + b + 3) * g0;
+  real p1 = ((a + b + 2) * x / 2 + (a - b) / 2) / r_sqrt(g1);
   if (n == 1) return p1;
-  double aold = 2.0 / (2 + a + b) * std::sqrt((a + 1) * (b + 1) / (a + b + 3));
+  real aold = 2.0 / (2 + a + b) * r_sqrt((a + 1) * (b + 1) / (a + b + 3));
   for (int i = 1; i < n; i++) {
-    double h1 = 2.0 * i + a + b;
-    double anew = 2.0 / (h1 + 2) * std::sqrt((i + 1) * (i + 1 + a + b) * (i + 1 + a) * (i + 1 + b) / (h1 + 1) / (h1 + 3));
-    double bnew = -(a * a - b * b) / h1 / (h1 + 2);
-    double p2 = (-aold * p0 + (x - bnew) * p1) / anew;
+    real h1 = 2.0 * i + a + b;
+    real anew = 2.0 / (h1 + 2) * r_sqrt((i + 1) * (i + 1 + a + b) * (i + 1 + a) * (i + 1 + b) / (h1 + 1) / (h1 + 3));
+    real bnew = -(a * a - b * b) / h1 / (h1 + 2);
+    real p2 = (-aold * p0 + (x - bnew) * p1) / anew;
     p0 = p1;
     p1 = p2;
     aold = anew;
   }
   return p1;
 }
-static double jacobi_d(double x, double a, double b, int n) {
-  return n == 0 ? 0.0 : std::sqrt(n * (n + a + b + 1)) * jacobi(x, a + 1, b + 1, n - 1);
+static real jacobi_d(real x, real a, real b, int n) {
+  return n == 0 ? 0.0 : r_sqrt(n * (n + a + b + 1)) * jacobi(x, a + 1, b + 1, n - 1);
 }
 
 // PKD mode (i, j) and its (r, s) derivatives at a point of the biunit triangle.
-static void pkd_mode(int i, int j, double r, double s, double& v, double& vr, double& vs) {
-  double a = (std::fabs(s - 1.0) > 1e-14) ? 2.0 * (1.0 + r) / (1.0 - s) - 1.0 : -1.0, b = s;
-  double fa = jacobi(a, 0, 0, i), dfa = jacobi_d(a, 0, 0, i);
-  double gb = jacobi(b, 2 * i + 1, 0, j), dgb = jacobi_d(b, 2 * i + 1, 0, j);
-  double hb = 0.5 * (1.0 - b);
-  v = std::sqrt(2.0) * fa * gb * std::pow(1.0 - b, i);
-  double dr = dfa * gb, ds = dfa * gb * 0.5 * (1.0 + a);
-  if (i > 0) { dr *= std::pow(hb, i - 1); ds *= std::pow(hb, i - 1); }
-  double tmp = dgb * std::pow(hb, i);
-  if (i > 0) tmp -= 0.5 * i * gb * std::pow(hb, i - 1);
+static void pkd_mode(int i, int j, real r, real s, real& v, real& vr, real& vs) {
+  real a = (r_fabs(s - 1.0) > 1e-14) ? 2.0 * (1.0 + r) / (1.0 - s) - 1.0 : -1.0, b = s;
+  real fa = jacobi(a, 0, 0, i), dfa = jacobi_d(a, 0, 0, i);
+  real gb = jacobi(b, 2 * i + 1, 0, j), dgb = jacobi_d(b, 2 * i + 1, 0, j);
+  real hb = 0.5 * (1.0 - b);
+  v = r_sqrt(2.0) * fa * gb * r_pow(1.0 - b, i);
+  real dr = dfa * gb, ds = dfa * gb * 0.5 * (1.0 + a);
+  if (i > 0) { dr *= r_pow(hb, i - 1); ds *= r_pow(hb, i - 1); }
+  real tmp = dgb * r_pow(hb, i);
+  if (i > 0) tmp -= 0.5 * i * gb * r_pow(hb, i - 1);
   ds += fa * tmp;
-  const double sc = std::pow(2.0, i + 0.5);
+  const real sc = r_pow(2.0, i + 0.5);
   vr = dr * sc;
   vs = ds * sc;
 }
 
 // Warp & blend lattice of degree N on the reference triangle (0,0),(1,0),(0,1):
 // Np = (N+1)(N+2)/2 points, bottom row first (eta = 0, xi ascending).
-static vector<double> warp_blend_tri(int N) {
-  static const double alpopt[15] = {0.0000, 0.0000, 1.4152, 0.1001, 0.2751, 0.9800, 1.0999, 1.2832,
+static vector<real> warp_blend_tri(int N) {
+  static const real alpopt[15] = {0.0000, 0.0000, 1.4152, 0.1001, 0.2751, 0.9800, 1.0999, 1.2832,
                                     1.3648, 1.4773, 1.4959, 1.5743, 1.5770, 1.6223, 1.6258};
-  const double alpha = N < 16 ? alpopt[N - 1] : 5.0 / 3.0;
-  vector<double> gll(N + 1);
+  const real alpha = N < 16 ? alpopt[N - 1] : 5.0 / 3.0;
+  vector<real> gll(N + 1);
   gauss_lobatto(N, gll.data());
-  auto warpf = [&](double r) {
+  auto warpf = [&](real r) {
     // interpolant on equispaced nodes of the GLL displacement, divided by 1 - r^2
-    double w = 0.0;
+    real w = 0.0;
     for (int i = 0; i <= N; i++) {
-      double xi_eq = -1.0 + 2.0 * i / N, l = 1.0;
+      real xi_eq = -1.0 + 2.0 * i / N, l = 1.0;
       for (int j = 0; j <= N; j++)
         if (j != i) l *= (r - (-1.0 + 2.0 * j / N)) / (xi_eq - (-1.0 + 2.0 * j / N));
       w += (gll[i] - xi_eq) * l;
     }
-    return std::fabs(r) < 1.0 - 1e-10 ? w / (1.0 - r * r) : 0.0;
+    return r_fabs(r) < 1.0 - 1e-10 ? w / (1.0 - r * r) : 0.0;
   };
-  vector<double> out;
-  const double c2 = std::cos(2 * M_PI / 3), s2 = std::sin(2 * M_PI / 3);
-  const double c4 = std::cos(4 * M_PI / 3), s4 = std::sin(4 * M_PI / 3);
+  vector<real> out;
+  const real c2 = r_cos(2 * R_PI / 3), s2 = r_sin(2 * R_PI / 3);
+  const real c4 = r_cos(4 * R_PI / 3), s4 = r_sin(4 * R_PI / 3);
   for (int n = 0; n <= N; n++)
     for (int m = 0; m <= N - n; m++) {
-      double L1 = (double)n / N, L3 = (double)m / N, L2 = 1.0 - L1 - L3;
-      double x = -L2 + L3, y = (-L2 - L3 + 2 * L1) / std::sqrt(3.0);
-      double w1 = 4 * L2 * L3 * warpf(L3 - L2) * (1 + (alpha * L1) * (alpha * L1));
-      double w2 = 4 * L1 * L3 * warpf(L1 - L3) * (1 + (alpha * L2) * (alpha * L2));
-      double w3 = 4 * L1 * L2 * warpf(L2 - L1) * (1 + (alpha * L3) * (alpha * L3));
+      real L1 = (real)n / N, L3 = (real)m / N, L2 = 1.0 - L1 - L3;
+      real x = -L2 + L3, y = (-L2 - L3 + 2 * L1) / r_sqrt(3.0);
+      real w1 = 4 * L2 * L3 * warpf(L3 - L2) * (1 + (alpha * L1) * (alpha * L1));
+      real w2 = 4 * L1 * L3 * warpf(L1 - L3) * (1 + (alpha * L2) * (alpha * L2));
+      real w3 = 4 * L1 * L2 * warpf(L2 - L1) * (1 + (alpha * L3) * (alpha * L3));
       x += w1 + c2 * w2 + c4 * w3;
       y += s2 * w2 + s4 * w3;
       // equilateral -> biunit (r, s) -> reference (xi, eta)
-      double b1 = (std::sqrt(3.0) * y + 1) / 3, b2 = (-3 * x - std::sqrt(3.0) * y + 2) / 6,
-             b3 = (3 * x - std::sqrt(3.0) * y + 2) / 6;
-      double r = -b2 + b3 - b1, s = -b2 - b3 + b1;
+      real b1 = (r_sqrt(3.0) * y + 1) / 3, b2 = (-3 * x - r_sqrt(3.0) * y + 2) / 6,
+             b3 = (3 * x - r_sqrt(3.0) * y + 2) / 6;
+      real r = -b2 + b3 - b1, s = -b2 - b3 + b1;
       out.push_back(0.5 * (1 + r));
       out.push_back(0.5 * (1 + s));
     }
@@ -308,19 +350,19 @@ static vector<double> warp_blend_tri(int N) {
 }
 
 // Inverse of a dense n x n matrix (Gauss-Jordan, partial pivoting).
-static vector<double> invert(vector<double> A, int n) {
-  vector<double> X(n * n, 0.0);
+static vector<real> invert(vector<real> A, int n) {
+  vector<real> X(n * n, 0.0);
   for (int i = 0; i < n; i++) X[i * n + i] = 1.0;
   for (int c = 0; c < n; c++) {
     int piv = c;
     for (int r = c + 1; r < n; r++)
-      if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+      if (r_fabs(A[r * n + c]) > r_fabs(A[piv * n + c])) piv = r;
     for (int k = 0; k < n; k++) { std::swap(A[c * n + k], A[piv * n + k]); std::swap(X[c * n + k], X[piv * n + k]); }
-    double inv = 1.0 / A[c * n + c];
+    real inv = 1.0 / A[c * n + c];
     for (int k = 0; k < n; k++) { A[c * n + k] *= inv; X[c * n + k] *= inv; }
     for (int r = 0; r < n; r++) {
       if (r == c) continue;
-      double f = A[r * n + c];
+      real f = A[r * n + c];
       if (f == 0.0) continue;
       for (int k = 0; k < n; k++) { A[r * n + k] -= f * A[c * n + k]; X[r * n + k] -= f * X[c * n + k]; }
     }
@@ -331,17 +373,17 @@ static vector<double> invert(vector<double> A, int n) {
 // Lagrange basis of degree N on the warp & blend lattice: phi_k = sum_m psi_m Vinv[m][k].
 struct TriLagrange {
   int N = 0, card = 1;
-  vector<double> vinv;
+  vector<real> vinv;
   void init(int n) {
     N = n;
     card = (n + 1) * (n + 2) / 2;
     if (n == 0) return;
-    vector<double> X = warp_blend_tri(n), V((size_t)card * card);
+    vector<real> X = warp_blend_tri(n), V((size_t)card * card);
     for (int p = 0; p < card; p++) {
       int m = 0;
       for (int i = 0; i <= n; i++)
         for (int j = 0; j <= n - i; j++, m++) {
-          double v, vr, vs;
+          real v, vr, vs;
           pkd_mode(i, j, 2 * X[2 * p] - 1, 2 * X[2 * p + 1] - 1, v, vr, vs);
           V[(size_t)p * card + m] = v;
         }
@@ -349,20 +391,20 @@ struct TriLagrange {
     vinv = invert(V, card);
   }
   // values and reference (xi, eta) gradients of all card functions
-  void eval(const double* xi, double* val, double* grad) const {
+  void eval(const real* xi, real* val, real* grad) const {
     if (N == 0) {
       if (val) val[0] = 1.0;
       if (grad) { grad[0] = 0.0; grad[1] = 0.0; }
       return;
     }
-    vector<double> pv(card), pr(card), ps(card);
+    vector<real> pv(card), pr(card), ps(card);
     int m = 0;
     for (int i = 0; i <= N; i++)
       for (int j = 0; j <= N - i; j++, m++) pkd_mode(i, j, 2 * xi[0] - 1, 2 * xi[1] - 1, pv[m], pr[m], ps[m]);
     for (int k = 0; k < card; k++) {
-      double v = 0, gx = 0, gy = 0;
+      real v = 0, gx = 0, gy = 0;
       for (int mm = 0; mm < card; mm++) {
-        double c = vinv[(size_t)mm * card + k];
+        real c = vinv[(size_t)mm * card + k];
         v += pv[mm] * c;
         gx += pr[mm] * c;
         gy += ps[mm] * c;
@@ -374,9 +416,9 @@ struct TriLagrange {
 };
 
 // Modal RT_n basis on the reference triangle: values (2 per function) and divergence.
-static void tri_rt_eval(int n, const double* xi, double* val, double* div) {
+static void tri_rt_eval(int n, const real* xi, real* val, real* div) {
   const int np = n * (n + 1) / 2;  // dim P_{n-1}
-  vector<double> pv(np), pr(np), ps(np);
+  vector<real> pv(np), pr(np), ps(np);
   int m = 0;
   for (int i = 0; i <= n - 1; i++)
     for (int j = 0; j <= n - 1 - i; j++, m++) pkd_mode(i, j, 2 * xi[0] - 1, 2 * xi[1] - 1, pv[m], pr[m], ps[m]);
@@ -387,7 +429,7 @@ static void tri_rt_eval(int n, const double* xi, double* val, double* div) {
       if (div) div[dof] = 2 * (c == 0 ? pr[k] : ps[k]);
     }
   for (int j = 0; j < n; j++, dof++) {
-    double v, vr, vs;  // PKD polynomial of exact degree n-1; d/dxi = 2 d/dr
+    real v, vr, vs;  // PKD polynomial of exact degree n-1; d/dxi = 2 d/dr
     pkd_mode(n - 1 - j, j, 2 * xi[0] - 1, 2 * xi[1] - 1, v, vr, vs);
     if (val) { val[2 * dof] = xi[0] * v; val[2 * dof + 1] = xi[1] * v; }
     if (div) div[dof] = 2 * v + 2 * (xi[0] * vr + xi[1] * vs);
@@ -401,7 +443,7 @@ struct Basis {
   Nodal1D closed, open;            // 1D families
   TriLagrange tri;                 // triangle HGRAD
   // Tabulate at point xi: val[card*vdim], grad[card*d] (HGRAD-type), div[card]
-  void eval(const double* xi, double* val, double* grad, double* div) const;
+  void eval(const real* xi, real* val, real* grad, real* div) const;
 };
 
 // Triangle bases are tabulated through a monomial-coefficient representation.
@@ -409,7 +451,7 @@ struct TriPoly {
   // dofs: coefficients in the monomial basis x^a y^b, a+b <= deg
   int deg = 0;
   vector<std::pair<int, int>> mono;
-  vector<double> coef;  // card x nmono (scalar) or card x 2 x nmono (vector)
+  vector<real> coef;  // card x nmono (scalar) or card x 2 x nmono (vector)
 };
 
 static int tensor_card(const Basis& b) {
@@ -450,7 +492,7 @@ static Basis make_basis(int topo, int space, int n, int ncomp = 1) {
   return b;
 }
 
-void Basis::eval(const double* xi, double* val, double* grad, double* div) const {
+void Basis::eval(const real* xi, real* val, real* grad, real* div) const {
   int d_ = d;
   if (topo == DPG_TOPO_TRI) {
     if (space == DPG_SPACE_HDIV) {
@@ -458,7 +500,7 @@ void Basis::eval(const double* xi, double* val, double* grad, double* div) const
       return;
     }
     const int nper = tri.card;
-    vector<double> v(nper), gr(2 * nper);
+    vector<real> v(nper), gr(2 * nper);
     tri.eval(xi, v.data(), gr.data());
     for (int c = 0; c < ncomp; c++)
       for (int k = 0; k < nper; k++) {
@@ -472,19 +514,19 @@ void Basis::eval(const double* xi, double* val, double* grad, double* div) const
     int m = closed.size();
     int nper = 1;
     for (int k = 0; k < d_; k++) nper *= m;
-    double v1[3][16], d1[3][16];
+    real v1[3][16], d1[3][16];
     for (int k = 0; k < d_; k++)
       for (int i = 0; i < m; i++) closed.eval(i, xi[k], v1[k][i], d1[k][i]);
     for (int c = 0; c < ncomp; c++) {
       for (int idx = 0; idx < nper; idx++) {
         int ii[3] = {idx % m, (idx / m) % m, idx / (m * m)};
-        double v = 1.0;
+        real v = 1.0;
         for (int k = 0; k < d_; k++) v *= v1[k][ii[k]];
         int dof = c * nper + idx;
         if (val) val[dof] = v;
         if (grad) {
           for (int k = 0; k < d_; k++) {
-            double g = d1[k][ii[k]];
+            real g = d1[k][ii[k]];
             for (int j = 0; j < d_; j++) if (j != k) g *= v1[j][ii[j]];
             grad[dof * d_ + k] = g;
           }
@@ -497,7 +539,7 @@ void Basis::eval(const double* xi, double* val, double* grad, double* div) const
   // and open (degree n-1) in the other directions; dofs component-major,
   // x fastest inside a component.
   int c1 = closed.size(), o1 = open.size();
-  double cv[3][16], cd[3][16], ov[3][16], od[3][16];
+  real cv[3][16], cd[3][16], ov[3][16], od[3][16];
   for (int k = 0; k < d_; k++) {
     for (int i = 0; i < c1; i++) closed.eval(i, xi[k], cv[k][i], cd[k][i]);
     for (int i = 0; i < o1; i++) open.eval(i, xi[k], ov[k][i], od[k][i]);
@@ -512,9 +554,9 @@ void Basis::eval(const double* xi, double* val, double* grad, double* div) const
       int ii[3];
       int r = idx;
       for (int k = 0; k < d_; k++) { ii[k] = r % ext[k]; r /= ext[k]; }
-      double f = 1.0, df = 1.0;
+      real f = 1.0, df = 1.0;
       for (int k = 0; k < d_; k++) {
-        double vv = (k == comp) ? cv[k][ii[k]] : ov[k][ii[k]];
+        real vv = (k == comp) ? cv[k][ii[k]] : ov[k][ii[k]];
         f *= vv;
         if (k == comp) df *= cd[k][ii[k]]; else df *= vv;
       }
@@ -531,8 +573,8 @@ void Basis::eval(const double* xi, double* val, double* grad, double* div) const
 
 struct Rule {
   int dim = 0;
-  vector<double> pts;  // npts x dim
-  vector<double> wts;
+  vector<real> pts;  // npts x dim
+  vector<real> wts;
   int npts() const { return (int)wts.size(); }
 };
 
@@ -540,7 +582,7 @@ static int gauss_points_for_degree(int degree) { return degree / 2 + 1; }
 
 static Rule tensor_gauss(int dim, int degree) {
   int n = gauss_points_for_degree(degree);
-  vector<double> x(n), w(n);
+  vector<real> x(n), w(n);
   gauss_legendre(n, x.data(), w.data());
   Rule r;
   r.dim = dim;
@@ -550,7 +592,7 @@ static Rule tensor_gauss(int dim, int degree) {
   r.wts.resize(total);
   for (int idx = 0; idx < total; idx++) {
     int rr = idx;
-    double wt = 1.0;
+    real wt = 1.0;
     for (int k = 0; k < dim; k++) {
       int i = rr % n; rr /= n;
       r.pts[idx * dim + k] = x[i];
@@ -567,14 +609,14 @@ static Rule tensor_gauss(int dim, int degree) {
 // xi = u (1 - v), eta = v, weight w_u w_v (1 - v) / 4 on [0,1]^2, u fastest.
 static Rule tri_rule(int degree) {
   const int nu = degree / 2 + 1, nv = (degree + 1) / 2 + 1;
-  vector<double> xu(nu), wu(nu), xv(nv), wv(nv);
+  vector<real> xu(nu), wu(nu), xv(nv), wv(nv);
   gauss_legendre(nu, xu.data(), wu.data());
   gauss_legendre(nv, xv.data(), wv.data());
   Rule r;
   r.dim = 2;
   for (int j = 0; j < nv; j++)
     for (int i = 0; i < nu; i++) {
-      double u = 0.5 * (1 + xu[i]), v = 0.5 * (1 + xv[j]);
+      real u = 0.5 * (1 + xu[i]), v = 0.5 * (1 + xv[j]);
       r.pts.push_back(u * (1 - v));
       r.pts.push_back(v);
       r.wts.push_back(0.25 * wu[i] * wv[j] * (1 - v));
@@ -597,10 +639,10 @@ struct VarLayout {
 // Reference tabulation of one basis at one point set.
 struct RefTab {
   int card = 0, vdim = 1, d = 0;
-  vector<double> val, grad, div;  // (npts, card, vdim), (npts, card, d), (npts, card)
+  vector<real> val, grad, div;  // (npts, card, vdim), (npts, card, d), (npts, card)
 };
 
-static RefTab tabulate(const Basis& b, const double* pts, int npts) {
+static RefTab tabulate(const Basis& b, const real* pts, int npts) {
   RefTab t;
   t.card = b.card; t.d = b.d; t.vdim = b.rank ? b.d : 1;
   t.val.assign((size_t)npts * t.card * t.vdim, 0.0);
@@ -623,7 +665,7 @@ struct Plan {
   int d = 0, N = 0, M = 0, nf = 0, nt = 0;
   vector<VarLayout> tv, rv;  // test vars, trial vars
   Rule rG, rB, rS;           // rS in side parameter coordinates
-  vector<vector<double>> side_pts;  // per side: Q_side x d volume reference points
+  vector<vector<real>> side_pts;  // per side: Q_side x d volume reference points
   int nIPterms = 0;
   vector<int> ip_ncomp;
   vector<int> is_field;  // per trial dof
@@ -694,16 +736,16 @@ static bool build_plan(Plan& P, const dpg_bucket_desc* desc) {
     auto& sp = P.side_pts[s];
     sp.assign(P.rS.npts() * P.d, 0.0);
     for (int q = 0; q < P.rS.npts(); q++) {
-      const double* t = &P.rS.pts[q * (P.d - 1)];
+      const real* t = &P.rS.pts[q * (P.d - 1)];
       if (P.d == 2) {
-        const double* a = P.topo.v[P.topo.sv[s][0]];
-        const double* b = P.topo.v[P.topo.sv[s][1]];
+        const real* a = P.topo.v[P.topo.sv[s][0]];
+        const real* b = P.topo.v[P.topo.sv[s][1]];
         for (int k = 0; k < 2; k++) sp[q * 2 + k] = 0.5 * (1 - t[0]) * a[k] + 0.5 * (1 + t[0]) * b[k];
       } else {
-        double Nq[4] = {0.25 * (1 - t[0]) * (1 - t[1]), 0.25 * (1 + t[0]) * (1 - t[1]),
+        real Nq[4] = {0.25 * (1 - t[0]) * (1 - t[1]), 0.25 * (1 + t[0]) * (1 - t[1]),
                         0.25 * (1 + t[0]) * (1 + t[1]), 0.25 * (1 - t[0]) * (1 + t[1])};
         for (int k = 0; k < 3; k++) {
-          double x = 0;
+          real x = 0;
           for (int a = 0; a < 4; a++) x += Nq[a] * P.topo.v[P.topo.sv[s][a]][k];
           sp[q * 3 + k] = x;
         }
@@ -739,17 +781,17 @@ static bool build_plan(Plan& P, const dpg_bucket_desc* desc) {
 
 // Geometry at a reference point.
 struct Geo {
-  double J[3][3], Ji[3][3], det;
+  real J[3][3], Ji[3][3], det;
 };
 
-static void geometry(const Plan& P, const double* nodes, const double* xi, Geo& g) {
+static void geometry(const Plan& P, const real* nodes, const real* xi, Geo& g) {
   int d = P.d, nv = P.topo.nv;
-  double Nv[8], dN[24];
+  real Nv[8], dN[24];
   geom_shape(P.topo, xi, Nv, dN);
   for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) g.J[i][j] = (i == j && i >= d) ? 1.0 : 0.0;
   for (int i = 0; i < d; i++)
     for (int j = 0; j < d; j++) {
-      double s = 0;
+      real s = 0;
       for (int a = 0; a < nv; a++) s += nodes[a * d + i] * dN[a * d + j];
       g.J[i][j] = s;
     }
@@ -758,12 +800,12 @@ static void geometry(const Plan& P, const double* nodes, const double* xi, Geo& 
     g.Ji[0][0] = g.J[1][1] / g.det; g.Ji[0][1] = -g.J[0][1] / g.det;
     g.Ji[1][0] = -g.J[1][0] / g.det; g.Ji[1][1] = g.J[0][0] / g.det;
   } else {
-    double (*A)[3] = g.J;
-    double c00 = A[1][1] * A[2][2] - A[1][2] * A[2][1];
-    double c01 = A[1][2] * A[2][0] - A[1][0] * A[2][2];
-    double c02 = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+    real (*A)[3] = g.J;
+    real c00 = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+    real c01 = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+    real c02 = A[1][0] * A[2][1] - A[1][1] * A[2][0];
     g.det = A[0][0] * c00 + A[0][1] * c01 + A[0][2] * c02;
-    double id = 1.0 / g.det;
+    real id = 1.0 / g.det;
     g.Ji[0][0] = c00 * id;
     g.Ji[1][0] = c01 * id;
     g.Ji[2][0] = c02 * id;
@@ -777,56 +819,56 @@ static void geometry(const Plan& P, const double* nodes, const double* xi, Geo& 
 }
 
 // Side measure factor and outward unit normal at side point q of side s.
-static void side_geometry(const Plan& P, const Geo& g, int s, int q, double& meas, double* n) {
+static void side_geometry(const Plan& P, const Geo& g, int s, int q, real& meas, real* n) {
   int d = P.d;
   if (d == 2) {
-    const double* a = P.topo.v[P.topo.sv[s][0]];
-    const double* b = P.topo.v[P.topo.sv[s][1]];
-    double tr[2] = {0.5 * (b[0] - a[0]), 0.5 * (b[1] - a[1])};
-    double T[2] = {g.J[0][0] * tr[0] + g.J[0][1] * tr[1], g.J[1][0] * tr[0] + g.J[1][1] * tr[1]};
-    meas = std::sqrt(T[0] * T[0] + T[1] * T[1]);
+    const real* a = P.topo.v[P.topo.sv[s][0]];
+    const real* b = P.topo.v[P.topo.sv[s][1]];
+    real tr[2] = {0.5 * (b[0] - a[0]), 0.5 * (b[1] - a[1])};
+    real T[2] = {g.J[0][0] * tr[0] + g.J[0][1] * tr[1], g.J[1][0] * tr[0] + g.J[1][1] * tr[1]};
+    meas = r_sqrt(T[0] * T[0] + T[1] * T[1]);
     n[0] = T[1] / meas; n[1] = -T[0] / meas; n[2] = 0;
   } else {
-    const double* t = &P.rS.pts[q * 2];
-    double dNs[4] = {-0.25 * (1 - t[1]), 0.25 * (1 - t[1]), 0.25 * (1 + t[1]), -0.25 * (1 + t[1])};
-    double dNt[4] = {-0.25 * (1 - t[0]), -0.25 * (1 + t[0]), 0.25 * (1 + t[0]), 0.25 * (1 - t[0])};
-    double rs[3] = {0, 0, 0}, rt[3] = {0, 0, 0};
+    const real* t = &P.rS.pts[q * 2];
+    real dNs[4] = {-0.25 * (1 - t[1]), 0.25 * (1 - t[1]), 0.25 * (1 + t[1]), -0.25 * (1 + t[1])};
+    real dNt[4] = {-0.25 * (1 - t[0]), -0.25 * (1 + t[0]), 0.25 * (1 + t[0]), 0.25 * (1 - t[0])};
+    real rs[3] = {0, 0, 0}, rt[3] = {0, 0, 0};
     for (int a = 0; a < 4; a++)
       for (int k = 0; k < 3; k++) {
         rs[k] += dNs[a] * P.topo.v[P.topo.sv[s][a]][k];
         rt[k] += dNt[a] * P.topo.v[P.topo.sv[s][a]][k];
       }
-    double Ts[3], Tt[3];
+    real Ts[3], Tt[3];
     for (int i = 0; i < 3; i++) {
       Ts[i] = g.J[i][0] * rs[0] + g.J[i][1] * rs[1] + g.J[i][2] * rs[2];
       Tt[i] = g.J[i][0] * rt[0] + g.J[i][1] * rt[1] + g.J[i][2] * rt[2];
     }
-    double c[3] = {Ts[1] * Tt[2] - Ts[2] * Tt[1], Ts[2] * Tt[0] - Ts[0] * Tt[2], Ts[0] * Tt[1] - Ts[1] * Tt[0]};
-    meas = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    real c[3] = {Ts[1] * Tt[2] - Ts[2] * Tt[1], Ts[2] * Tt[0] - Ts[0] * Tt[2], Ts[0] * Tt[1] - Ts[1] * Tt[0]};
+    meas = r_sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
     for (int k = 0; k < 3; k++) n[k] = c[k] / meas;
   }
 }
 
 // Physical value of test op for all dofs of a test var at point q of a table.
 // out[i] for i in [0, card)
-static void test_op_values(const Plan& P, const RefTab& T, int q, int op, const Geo& g, const double* nrm,
-                           double* out) {
+static void test_op_values(const Plan& P, const RefTab& T, int q, int op, const Geo& g, const real* nrm,
+                           real* out) {
   int d = P.d, card = T.card;
   bool vec = T.vdim > 1;
-  const double* val = &T.val[(size_t)q * card * T.vdim];
+  const real* val = &T.val[(size_t)q * card * T.vdim];
   for (int i = 0; i < card; i++) {
-    double r = 0;
+    real r = 0;
     if (!vec) {
       if (op == DPG_OP_VALUE) r = val[i];
       else if (op >= DPG_OP_DX && op <= DPG_OP_DZ) {
-        const double* grad = &T.grad[((size_t)q * card + i) * d];
+        const real* grad = &T.grad[((size_t)q * card + i) * d];
         int c = op - DPG_OP_DX;
         for (int j = 0; j < d; j++) r += g.Ji[j][c] * grad[j];  // (J^-T grad)_c
       }
     } else {
-      double pv[3] = {0, 0, 0};
+      real pv[3] = {0, 0, 0};
       for (int c = 0; c < d; c++) {
-        double s = 0;
+        real s = 0;
         for (int j = 0; j < d; j++) s += g.J[c][j] * val[i * d + j];
         pv[c] = s / g.det;
       }
@@ -839,23 +881,23 @@ static void test_op_values(const Plan& P, const RefTab& T, int q, int op, const 
 }
 
 // Trial values of field var L (op VALUE or component) at point q of a table.
-static void field_values(const VarLayout& L, const RefTab& T, int q, int op, double* out) {
+static void field_values(const VarLayout& L, const RefTab& T, int q, int op, real* out) {
   const Basis& b = L.basis;
-  const double* val = &T.val[(size_t)q * T.card];
+  const real* val = &T.val[(size_t)q * T.card];
   int per = b.card / b.ncomp;
   int comp = (b.ncomp > 1) ? (op - DPG_OP_X) : 0;
   for (int i = 0; i < b.card; i++) out[i] = (i / per == comp) ? val[i] : 0.0;
 }
 
-static inline double slotval(const double* coeff_cell, int P_total, int slot, int p) {
+static inline real slotval(const real* coeff_cell, int P_total, int slot, int p) {
   return slot < 0 ? 1.0 : coeff_cell[slot * P_total + p];
 }
 
 struct CellOut {
-  vector<double> G, B, F;  // G NxN, B MxN (row = trial), F N
+  vector<real> G, B, F;  // G NxN, B MxN (row = trial), F N
 };
 
-static void assemble_cell(const Plan& P, const double* nodes, const int8_t* parity, const double* coeff,
+static void assemble_cell(const Plan& P, const real* nodes, const int8_t* parity, const real* coeff,
                           CellOut& o) {
   int N = P.N, M = P.M, d = P.d;
   int QG = P.rG.npts(), QB = P.rB.npts(), QS = P.rS.npts();
@@ -863,49 +905,73 @@ static void assemble_cell(const Plan& P, const double* nodes, const int8_t* pari
   o.G.assign((size_t)N * N, 0.0);
   o.B.assign((size_t)M * N, 0.0);
   o.F.assign(N, 0.0);
-  double nrm0[3] = {0, 0, 0};
-  // ---- G: sum over IP terms/components of L L^T, weighted --------------------
+  real nrm0[3] = {0, 0, 0};
+  // ---- G, in the reference's order (IP.cpp:238-244 -> LinearTerm.cpp:470-606):
+  // for each graph-norm term, for each (u var, v var) pair of that term, the
+  // weighted u values are contracted with the v values over (point, component) in
+  // one product (FunctionSpaceTools::integrate, COMP_BLAS) and the block is then
+  // added into G.  The order matters at h = 1/48: summing every term's products in
+  // one running sum per entry is 3-4x further from the exact G's factorisation.
   {
     int nT = 0;
-    for (int t = 0; t < P.nIPterms; t++) nT += P.ip_ncomp[t];
-    vector<double> Lm((size_t)nT * N);
-    vector<double> tmp(N);
+    vector<int> row0(P.nIPterms + 1, 0);
+    for (int t = 0; t < P.nIPterms; t++) { row0[t] = nT; nT += P.ip_ncomp[t]; }
+    row0[P.nIPterms] = nT;
+    // L[q][row][N]: term-component rows of every point; wm[q] = w |J|
+    vector<real> Lm((size_t)QG * nT * N, 0.0), wm(QG);
+    vector<real> tmp(N);
     for (int q = 0; q < QG; q++) {
-      const double* xi = &P.rG.pts[q * d];
+      const real* xi = &P.rG.pts[q * d];
       Geo g;
       geometry(P, nodes, xi, g);
-      double wm = P.rG.wts[q] * g.det;
-      std::fill(Lm.begin(), Lm.end(), 0.0);
+      wm[q] = P.rG.wts[q] * g.det;
+      real* Lq = &Lm[(size_t)q * nT * N];
       for (auto& e : P.ip) {
-        int row = 0;
-        for (int t = 0; t < e.term; t++) row += P.ip_ncomp[t];
-        row += e.comp;
+        const int row = row0[e.term] + e.comp;
         const VarLayout& L = P.tv[e.test_var];
         test_op_values(P, P.test_tab[e.test_var][0], q, e.test_op, g, nrm0, tmp.data());
-        double cf = e.coef * slotval(coeff, Ptot, e.slot, q);
-        for (int i = 0; i < L.ndofs; i++) Lm[(size_t)row * N + L.offset + i] += cf * tmp[i];
+        real cf = e.coef * slotval(coeff, Ptot, e.slot, q);
+        for (int i = 0; i < L.ndofs; i++) Lq[(size_t)row * N + L.offset + i] += cf * tmp[i];
       }
-      for (int r = 0; r < nT; r++) {
-        const double* Lr = &Lm[(size_t)r * N];
-        for (int i = 0; i < N; i++) {
-          double a = wm * Lr[i];
-          if (a == 0.0) continue;
-          double* Gi = &o.G[(size_t)i * N];
-          for (int j = 0; j <= i; j++) Gi[j] += a * Lr[j];
+    }
+    vector<real> wu;
+    for (int t = 0; t < P.nIPterms; t++) {
+      vector<int> vars;
+      for (auto& e : P.ip)
+        if (e.term == t && std::find(vars.begin(), vars.end(), e.test_var) == vars.end()) vars.push_back(e.test_var);
+      std::sort(vars.begin(), vars.end());
+      const int nc = P.ip_ncomp[t];
+      for (int u : vars) {
+        const VarLayout& U = P.tv[u];
+        // weighted u values (C, F, P, D) for this term: wu[i][q][c]
+        wu.assign((size_t)U.ndofs * QG * nc, 0.0);
+        for (int i = 0; i < U.ndofs; i++)
+          for (int q = 0; q < QG; q++)
+            for (int c = 0; c < nc; c++)
+              wu[((size_t)i * QG + q) * nc + c] = wm[q] * Lm[((size_t)q * nT + row0[t] + c) * N + U.offset + i];
+        for (int v : vars) {
+          const VarLayout& V = P.tv[v];
+          for (int i = 0; i < U.ndofs; i++)
+            for (int j = 0; j < V.ndofs; j++) {
+              real acc = 0.0;
+              const real* a = &wu[(size_t)i * QG * nc];
+              for (int q = 0; q < QG; q++)
+                for (int c = 0; c < nc; c++)
+                  acc += a[q * nc + c] * Lm[((size_t)q * nT + row0[t] + c) * N + V.offset + j];
+              o.G[(size_t)(U.offset + i) * N + V.offset + j] += acc;
+            }
         }
       }
     }
-    for (int i = 0; i < N; i++)
-      for (int j = i + 1; j < N; j++) o.G[(size_t)i * N + j] = o.G[(size_t)j * N + i];
   }
   // ---- B and F volume ------------------------------------------------------
   {
-    vector<double> tv(N), rvv(M);
+    vector<real> tv(N), rvv(M);
     for (int q = 0; q < QB; q++) {
-      const double* xi = &P.rB.pts[q * d];
+      const real* xi = &P.rB.pts[q * d];
       Geo g;
       geometry(P, nodes, xi, g);
-      double wm = P.rB.wts[q] * g.det;
+      real wm = P.rB.wts[q] * g.det;
       int p = QG + q;
       for (auto& t : P.bf) {
         if (t.boundary) continue;
@@ -913,40 +979,40 @@ static void assemble_cell(const Plan& P, const double* nodes, const int8_t* pari
         const VarLayout& RL = P.rv[t.trial_var];
         test_op_values(P, P.test_tab[t.test_var][1], q, t.test_op, g, nrm0, tv.data());
         field_values(RL, P.field_tab[t.trial_var][1], q, t.trial_op, rvv.data());
-        double cf = wm * t.coef * slotval(coeff, Ptot, t.slot, p);
+        real cf = wm * t.coef * slotval(coeff, Ptot, t.slot, p);
         for (int m = 0; m < RL.ndofs; m++) {
-          double a = cf * rvv[m];
+          real a = cf * rvv[m];
           if (a == 0.0) continue;
-          double* Bm = &o.B[(size_t)(RL.offset + m) * N + TL.offset];
+          real* Bm = &o.B[(size_t)(RL.offset + m) * N + TL.offset];
           for (int i = 0; i < TL.ndofs; i++) Bm[i] += a * tv[i];
         }
       }
       for (auto& r : P.rhs) {
         const VarLayout& TL = P.tv[r.test_var];
         test_op_values(P, P.test_tab[r.test_var][1], q, r.test_op, g, nrm0, tv.data());
-        double cf = wm * r.coef * slotval(coeff, Ptot, r.slot, p);
+        real cf = wm * r.coef * slotval(coeff, Ptot, r.slot, p);
         for (int i = 0; i < TL.ndofs; i++) o.F[TL.offset + i] += cf * tv[i];
       }
     }
   }
   // ---- B sides ---------------------------------------------------------------
   {
-    vector<double> tv(N), rvv(M);
+    vector<real> tv(N), rvv(M);
     for (int s = 0; s < P.topo.nsides; s++) {
       for (int q = 0; q < QS; q++) {
-        const double* xi = &P.side_pts[s][q * d];
+        const real* xi = &P.side_pts[s][q * d];
         Geo g;
         geometry(P, nodes, xi, g);
-        double meas, nrm[3];
+        real meas, nrm[3];
         side_geometry(P, g, s, q, meas, nrm);
-        double wm = P.rS.wts[q] * meas;
+        real wm = P.rS.wts[q] * meas;
         int p = QG + QB + s * QS + q;
         for (auto& t : P.bf) {
           if (!t.boundary) continue;
           const VarLayout& TL = P.tv[t.test_var];
           const VarLayout& RL = P.rv[t.trial_var];
           test_op_values(P, P.test_tab[t.test_var][2 + s], q, t.test_op, g, nrm, tv.data());
-          double cf = wm * t.coef * slotval(coeff, Ptot, t.slot, p);
+          real cf = wm * t.coef * slotval(coeff, Ptot, t.slot, p);
           if (t.normal_comp >= 0) cf *= nrm[t.normal_comp];
           int m0, mcount;
           if (RL.kind == DPG_VAR_FIELD) {
@@ -955,13 +1021,13 @@ static void assemble_cell(const Plan& P, const double* nodes, const int8_t* pari
           } else {
             const RefTab& TT = P.trace_tab[t.trial_var];
             for (int m = 0; m < RL.per_side; m++) rvv[m] = TT.val[(size_t)q * TT.card + m];
-            if (RL.kind == DPG_VAR_FLUX) cf *= (double)parity[s];
+            if (RL.kind == DPG_VAR_FLUX) cf *= (real)parity[s];
             m0 = RL.offset + s * RL.per_side; mcount = RL.per_side;
           }
           for (int m = 0; m < mcount; m++) {
-            double a = cf * rvv[m];
+            real a = cf * rvv[m];
             if (a == 0.0) continue;
-            double* Bm = &o.B[(size_t)(m0 + m) * N + TL.offset];
+            real* Bm = &o.B[(size_t)(m0 + m) * N + TL.offset];
             for (int i = 0; i < TL.ndofs; i++) Bm[i] += a * tv[i];
           }
         }
@@ -970,19 +1036,110 @@ static void assemble_cell(const Plan& P, const double* nodes, const int8_t* pari
   }
 }
 
+// The same quadrature as assemble_cell, returned as operator rows instead of sums
+// (used by the tests that emulate reduced-precision contractions term by term):
+//   G = sum_q wm[q] sum_rows L[q][row]^T L[q][row]   (row = graph-norm term component,
+//       rterm[row] its term),
+//   B = sum_r U[r]^T V[r]   (U: M trial values times weight, coefficient, normal
+//       component and parity; V: N test-operator values), F = sum_r fw[r] FV[r].
+// dims = {term-component rows, B rows, F rows}.
+static void cell_operators(const Plan& P, const real* nodes, const int8_t* parity, const real* coeff,
+                           vector<real>& L, vector<real>& wm, vector<int>& rterm, vector<real>& U,
+                           vector<real>& V, vector<real>& fw, vector<real>& FV) {
+  int N = P.N, M = P.M, d = P.d;
+  int QG = P.rG.npts(), QB = P.rB.npts(), QS = P.rS.npts();
+  int Ptot = QG + QB + P.topo.nsides * QS;
+  int nT = 0;
+  vector<int> row0(P.nIPterms + 1, 0);
+  rterm.clear();
+  for (int t = 0; t < P.nIPterms; t++) {
+    row0[t] = nT;
+    nT += P.ip_ncomp[t];
+    for (int c = 0; c < P.ip_ncomp[t]; c++) rterm.push_back(t);
+  }
+  L.assign((size_t)QG * nT * N, 0.0);
+  wm.assign(QG, 0.0);
+  real nrm0[3] = {0, 0, 0};
+  vector<real> tmp(N), rvv(M);
+  for (int q = 0; q < QG; q++) {
+    Geo g;
+    geometry(P, nodes, &P.rG.pts[q * d], g);
+    wm[q] = P.rG.wts[q] * g.det;
+    for (auto& e : P.ip) {
+      const VarLayout& TL = P.tv[e.test_var];
+      test_op_values(P, P.test_tab[e.test_var][0], q, e.test_op, g, nrm0, tmp.data());
+      real cf = e.coef * slotval(coeff, Ptot, e.slot, q);
+      for (int i = 0; i < TL.ndofs; i++) L[((size_t)q * nT + row0[e.term] + e.comp) * N + TL.offset + i] += cf * tmp[i];
+    }
+  }
+  U.clear(); V.clear(); fw.clear(); FV.clear();
+  auto push_row = [&](vector<real>& dst, int n) { dst.resize(dst.size() + n, 0.0); return dst.size() - n; };
+  for (int q = 0; q < QB; q++) {
+    Geo g;
+    geometry(P, nodes, &P.rB.pts[q * d], g);
+    real w = P.rB.wts[q] * g.det;
+    int p = QG + q;
+    for (auto& t : P.bf) {
+      if (t.boundary) continue;
+      const VarLayout& TL = P.tv[t.test_var];
+      const VarLayout& RL = P.rv[t.trial_var];
+      size_t u0 = push_row(U, M), v0 = push_row(V, N);
+      test_op_values(P, P.test_tab[t.test_var][1], q, t.test_op, g, nrm0, tmp.data());
+      field_values(RL, P.field_tab[t.trial_var][1], q, t.trial_op, rvv.data());
+      real cf = w * t.coef * slotval(coeff, Ptot, t.slot, p);
+      for (int m = 0; m < RL.ndofs; m++) U[u0 + RL.offset + m] = cf * rvv[m];
+      for (int i = 0; i < TL.ndofs; i++) V[v0 + TL.offset + i] = tmp[i];
+    }
+    for (auto& r : P.rhs) {
+      const VarLayout& TL = P.tv[r.test_var];
+      size_t v0 = push_row(FV, N);
+      test_op_values(P, P.test_tab[r.test_var][1], q, r.test_op, g, nrm0, tmp.data());
+      fw.push_back(w * r.coef * slotval(coeff, Ptot, r.slot, p));
+      for (int i = 0; i < TL.ndofs; i++) FV[v0 + TL.offset + i] = tmp[i];
+    }
+  }
+  for (int s = 0; s < P.topo.nsides; s++)
+    for (int q = 0; q < QS; q++) {
+      Geo g;
+      geometry(P, nodes, &P.side_pts[s][q * d], g);
+      real meas, nrm[3];
+      side_geometry(P, g, s, q, meas, nrm);
+      real w = P.rS.wts[q] * meas;
+      int p = QG + QB + s * QS + q;
+      for (auto& t : P.bf) {
+        if (!t.boundary) continue;
+        const VarLayout& TL = P.tv[t.test_var];
+        const VarLayout& RL = P.rv[t.trial_var];
+        size_t u0 = push_row(U, M), v0 = push_row(V, N);
+        test_op_values(P, P.test_tab[t.test_var][2 + s], q, t.test_op, g, nrm, tmp.data());
+        real cf = w * t.coef * slotval(coeff, Ptot, t.slot, p);
+        if (t.normal_comp >= 0) cf *= nrm[t.normal_comp];
+        if (RL.kind == DPG_VAR_FIELD) {
+          field_values(RL, P.field_tab[t.trial_var][2 + s], q, t.trial_op, rvv.data());
+          for (int m = 0; m < RL.ndofs; m++) U[u0 + RL.offset + m] = cf * rvv[m];
+        } else {
+          const RefTab& TT = P.trace_tab[t.trial_var];
+          if (RL.kind == DPG_VAR_FLUX) cf *= (real)parity[s];
+          for (int m = 0; m < RL.per_side; m++) U[u0 + RL.offset + s * RL.per_side + m] = cf * TT.val[(size_t)q * TT.card + m];
+        }
+        for (int i = 0; i < TL.ndofs; i++) V[v0 + TL.offset + i] = tmp[i];
+      }
+    }
+}
+
 // ----------------------------------------------------------------------------
 // Dense kernels, LAPACK semantics (column-major views)
 // ----------------------------------------------------------------------------
 
 // BF.cpp:924-1018.  G (N x N, symmetric; overwritten), B column-major N x M
 // (overwritten with L^-1 B), F (N; overwritten).  K row-major M x M, l (M).
-int factored_cholesky_solve(int N, int M, double* G, double* B, double* F, double* K, double* l) {
+int factored_cholesky_solve(int N, int M, real* G, real* B, real* F, real* K, real* l) {
   int result = 0;
   // DPOEQU
-  vector<double> s(N);
+  vector<real> s(N);
   int info = 0;
   {
-    double smin = G[0], amax = G[0];
+    real smin = G[0], amax = G[0];
     for (int i = 0; i < N; i++) {
       s[i] = G[i * N + i];
       smin = std::min(smin, s[i]);
@@ -991,22 +1148,22 @@ int factored_cholesky_solve(int N, int M, double* G, double* B, double* F, doubl
     if (smin <= 0) {
       for (int i = 0; i < N; i++) if (s[i] <= 0) { info = i + 1; break; }
     } else {
-      for (int i = 0; i < N; i++) s[i] = 1.0 / std::sqrt(s[i]);
+      for (int i = 0; i < N; i++) s[i] = 1.0 / r_sqrt(s[i]);
     }
   }
   (void)info;
   for (int i = 0; i < N; i++)
     for (int j = 0; j < N; j++) G[i * N + j] *= s[i] * s[j];
   // DPOTRF('L'), column-major A(i,j) = G[j*N+i]
-  auto A = [&](int i, int j) -> double& { return G[(size_t)j * N + i]; };
+  auto A = [&](int i, int j) -> real& { return G[(size_t)j * N + i]; };
   for (int j = 0; j < N; j++) {
-    double ajj = A(j, j);
+    real ajj = A(j, j);
     for (int k = 0; k < j; k++) ajj -= A(j, k) * A(j, k);
-    if (ajj <= 0.0 || std::isnan(ajj)) { result = j + 1; break; }
-    ajj = std::sqrt(ajj);
+    if (ajj <= 0.0 || r_isnan(ajj)) { result = j + 1; break; }
+    ajj = r_sqrt(ajj);
     A(j, j) = ajj;
     for (int i = j + 1; i < N; i++) {
-      double v = A(i, j);
+      real v = A(i, j);
       for (int k = 0; k < j; k++) v -= A(i, k) * A(j, k);
       A(i, j) = v / ajj;
     }
@@ -1017,11 +1174,11 @@ int factored_cholesky_solve(int N, int M, double* G, double* B, double* F, doubl
     for (int i = j; i < N; i++) A(i, j) /= s[i];
   // DTRSM L X = B  (B column-major N x M, ld N)
   for (int c = 0; c < M; c++) {
-    double* b = &B[(size_t)c * N];
+    real* b = &B[(size_t)c * N];
     for (int j = 0; j < N; j++) {
       if (b[j] != 0.0) {
         b[j] /= A(j, j);
-        double bj = b[j];
+        real bj = b[j];
         for (int i = j + 1; i < N; i++) b[i] -= bj * A(i, j);
       }
     }
@@ -1029,9 +1186,9 @@ int factored_cholesky_solve(int N, int M, double* G, double* B, double* F, doubl
   // DSYRK lower: K = W^T W, then mirror
   for (int i = 0; i < M; i++)
     for (int j = 0; j <= i; j++) {
-      double acc = 0;
-      const double* wi = &B[(size_t)i * N];
-      const double* wj = &B[(size_t)j * N];
+      real acc = 0;
+      const real* wi = &B[(size_t)i * N];
+      const real* wj = &B[(size_t)j * N];
       for (int k = 0; k < N; k++) acc += wi[k] * wj[k];
       K[(size_t)i * M + j] = acc;
       K[(size_t)j * M + i] = acc;
@@ -1040,14 +1197,14 @@ int factored_cholesky_solve(int N, int M, double* G, double* B, double* F, doubl
   for (int j = 0; j < N; j++) {
     if (F[j] != 0.0) {
       F[j] /= A(j, j);
-      double fj = F[j];
+      real fj = F[j];
       for (int i = j + 1; i < N; i++) F[i] -= fj * A(i, j);
     }
   }
   // l = W^T y
   for (int m = 0; m < M; m++) {
-    double acc = 0;
-    const double* w = &B[(size_t)m * N];
+    real acc = 0;
+    const real* w = &B[(size_t)m * N];
     for (int k = 0; k < N; k++) acc += w[k] * F[k];
     l[m] = acc;
   }
@@ -1057,25 +1214,25 @@ int factored_cholesky_solve(int N, int M, double* G, double* B, double* F, doubl
 // Epetra_SerialDenseSolver-style solve of D X = R (n x n, nrhs columns),
 // optional DGEEQU equilibration (threshold 0.1), LU with partial pivoting.
 // D row-major n x n (copied), R row-major n x nrhs (overwritten by X).
-static int lu_solve_equilibrated(int n, const double* Din, double* R, int nrhs) {
-  vector<double> A(Din, Din + (size_t)n * n);
-  vector<double> r(n, 0.0), c(n, 0.0);
-  const double smlnum = 2.2250738585072014e-308 / 2.220446049250313e-16;
-  const double bignum = 1.0 / smlnum;
-  double rcmin = bignum, rcmax = 0.0;
+static int lu_solve_equilibrated(int n, const real* Din, real* R, int nrhs) {
+  vector<real> A(Din, Din + (size_t)n * n);
+  vector<real> r(n, 0.0), c(n, 0.0);
+  const real smlnum = 2.2250738585072014e-308 / 2.220446049250313e-16;
+  const real bignum = 1.0 / smlnum;
+  real rcmin = bignum, rcmax = 0.0;
   for (int i = 0; i < n; i++) {
-    for (int j = 0; j < n; j++) r[i] = std::max(r[i], std::fabs(A[(size_t)i * n + j]));
+    for (int j = 0; j < n; j++) r[i] = std::max(r[i], r_fabs(A[(size_t)i * n + j]));
     rcmin = std::min(rcmin, r[i]);
     rcmax = std::max(rcmax, r[i]);
   }
   bool equil = false;
-  double rowcnd = 0, colcnd = 0;
+  real rowcnd = 0, colcnd = 0;
   if (rcmin > 0.0) {
     for (int i = 0; i < n; i++) r[i] = 1.0 / std::min(std::max(r[i], smlnum), bignum);
     rowcnd = std::max(rcmin, smlnum) / std::min(rcmax, bignum);
-    double ccmin = bignum, ccmax = 0.0;
+    real ccmin = bignum, ccmax = 0.0;
     for (int j = 0; j < n; j++) {
-      for (int i = 0; i < n; i++) c[j] = std::max(c[j], std::fabs(A[(size_t)i * n + j]) * r[i]);
+      for (int i = 0; i < n; i++) c[j] = std::max(c[j], r_fabs(A[(size_t)i * n + j]) * r[i]);
       ccmin = std::min(ccmin, c[j]);
       ccmax = std::max(ccmax, c[j]);
     }
@@ -1095,18 +1252,18 @@ static int lu_solve_equilibrated(int n, const double* Din, double* R, int nrhs) 
   vector<int> piv(n);
   for (int k = 0; k < n; k++) {
     int p = k;
-    double best = std::fabs(A[(size_t)k * n + k]);
+    real best = r_fabs(A[(size_t)k * n + k]);
     for (int i = k + 1; i < n; i++)
-      if (std::fabs(A[(size_t)i * n + k]) > best) { best = std::fabs(A[(size_t)i * n + k]); p = i; }
+      if (r_fabs(A[(size_t)i * n + k]) > best) { best = r_fabs(A[(size_t)i * n + k]); p = i; }
     piv[k] = p;
     if (best == 0.0) return k + 1;
     if (p != k) {
       for (int j = 0; j < n; j++) std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
       for (int j = 0; j < nrhs; j++) std::swap(R[(size_t)k * nrhs + j], R[(size_t)p * nrhs + j]);
     }
-    double inv = 1.0 / A[(size_t)k * n + k];
+    real inv = 1.0 / A[(size_t)k * n + k];
     for (int i = k + 1; i < n; i++) {
-      double f = A[(size_t)i * n + k] * inv;
+      real f = A[(size_t)i * n + k] * inv;
       A[(size_t)i * n + k] = f;
       if (f == 0.0) continue;
       for (int j = k + 1; j < n; j++) A[(size_t)i * n + j] -= f * A[(size_t)k * n + j];
@@ -1115,7 +1272,7 @@ static int lu_solve_equilibrated(int n, const double* Din, double* R, int nrhs) 
   }
   for (int k = n - 1; k >= 0; k--) {
     for (int j = 0; j < nrhs; j++) {
-      double v = R[(size_t)k * nrhs + j];
+      real v = R[(size_t)k * nrhs + j];
       for (int i = k + 1; i < n; i++) v -= A[(size_t)k * n + i] * R[(size_t)i * nrhs + j];
       R[(size_t)k * nrhs + j] = v / A[(size_t)k * n + k];
     }
@@ -1128,11 +1285,11 @@ static int lu_solve_equilibrated(int n, const double* Din, double* R, int nrhs) 
 }
 
 // CondensedDofInterpreter.cpp:1138-1192 on the local K (fields = is_field).
-int condense(int M, const int* is_field, const double* K, const double* l, double* S, double* s) {
+int condense(int M, const int* is_field, const real* K, const real* l, real* S, real* s) {
   vector<int> fi, ti;
   for (int i = 0; i < M; i++) (is_field[i] ? fi : ti).push_back(i);
   int nf = (int)fi.size(), nt = (int)ti.size();
-  vector<double> D((size_t)nf * nf), Bc((size_t)nf * nt), X, y(nf);
+  vector<real> D((size_t)nf * nf), Bc((size_t)nf * nt), X, y(nf);
   for (int a = 0; a < nf; a++) {
     for (int b = 0; b < nf; b++) D[(size_t)a * nf + b] = K[(size_t)fi[a] * M + fi[b]];
     for (int b = 0; b < nt; b++) Bc[(size_t)a * nt + b] = K[(size_t)fi[a] * M + ti[b]];
@@ -1147,28 +1304,48 @@ int condense(int M, const int* is_field, const double* K, const double* l, doubl
   }
   for (int a = 0; a < nt; a++) {
     for (int b = 0; b < nt; b++) {
-      double v = K[(size_t)ti[a] * M + ti[b]];
+      real v = K[(size_t)ti[a] * M + ti[b]];
       for (int k = 0; k < nf; k++) v -= Bc[(size_t)k * nt + a] * X[(size_t)k * nt + b];
       S[(size_t)a * nt + b] = v;
     }
-    double v = l[ti[a]];
+    real v = l[ti[a]];
     for (int k = 0; k < nf; k++) v -= Bc[(size_t)k * nt + a] * y[k];
     s[a] = v;
   }
   return err ? -err : 0;
 }
 
-}  // namespace orc
+}  // namespace ORC_NS
 
 // ----------------------------------------------------------------------------
-// C interface for the test harness
+// C interface for the test harness (double in, double out)
 // ----------------------------------------------------------------------------
 
-using namespace orc;
+using namespace ORC_NS;
+
+static vector<real> widen(const double* x, size_t n) {
+  vector<real> v(n);
+  for (size_t i = 0; i < n; i++) v[i] = (real)x[i];
+  return v;
+}
+
+template <class V>
+static void narrow(const V& v, double* out) {
+  for (size_t i = 0; i < v.size(); i++) out[i] = (double)v[i];
+}
 
 extern "C" {
 
-const char* orc_last_error(void) { return orc::g_err.c_str(); }
+const char* orc_last_error(void) { return g_err.c_str(); }
+
+// 0 for the FP64 build, 1 for the extended-precision (__float128) build.
+int orc_precision(void) {
+#ifdef ORC_QUAD
+  return 1;
+#else
+  return 0;
+#endif
+}
 
 void* orc_plan_create(const dpg_bucket_desc* desc) {
   Plan* p = new Plan();
@@ -1201,23 +1378,24 @@ int orc_assemble(void* pp, int C, const double* nodes, const int8_t* parity, con
   size_t cstride = (size_t)p->desc.n_slots * pi.n_points_total;
   auto work = [&](int c0, int c1) {
     CellOut o;
-    vector<double> Gw, Bw, Fw, Kc((size_t)M * M), lc(M);
+    vector<real> Kc((size_t)M * M), lc(M);
     for (int c = c0; c < c1; c++) {
-      assemble_cell(*p, nodes + (size_t)c * nv * d, parity + (size_t)c * ns,
-                    coeff ? coeff + c * cstride : nullptr, o);
-      if (G) std::copy(o.G.begin(), o.G.end(), G + (size_t)c * N * N);
-      if (B) std::copy(o.B.begin(), o.B.end(), B + (size_t)c * M * N);
-      if (F) std::copy(o.F.begin(), o.F.end(), F + (size_t)c * N);
+      vector<real> xn = widen(nodes + (size_t)c * nv * d, (size_t)nv * d);
+      vector<real> xc = coeff ? widen(coeff + c * cstride, cstride) : vector<real>();
+      assemble_cell(*p, xn.data(), parity + (size_t)c * ns, coeff ? xc.data() : nullptr, o);
+      if (G) narrow(o.G, G + (size_t)c * N * N);
+      if (B) narrow(o.B, B + (size_t)c * M * N);
+      if (F) narrow(o.F, F + (size_t)c * N);
       if (!K && !l && !S && !s && !info) continue;
       int r = factored_cholesky_solve(N, M, o.G.data(), o.B.data(), o.F.data(), Kc.data(), lc.data());
       if (r == 0 && (S || s)) {
-        vector<double> Sc((size_t)nt * nt), sc(nt);
+        vector<real> Sc((size_t)nt * nt), sc(nt);
         r = condense(M, p->is_field.data(), Kc.data(), lc.data(), Sc.data(), sc.data());
-        if (S) std::copy(Sc.begin(), Sc.end(), S + (size_t)c * nt * nt);
-        if (s) std::copy(sc.begin(), sc.end(), s + (size_t)c * nt);
+        if (S) narrow(Sc, S + (size_t)c * nt * nt);
+        if (s) narrow(sc, s + (size_t)c * nt);
       }
-      if (K) std::copy(Kc.begin(), Kc.end(), K + (size_t)c * M * M);
-      if (l) std::copy(lc.begin(), lc.end(), l + (size_t)c * M);
+      if (K) narrow(Kc, K + (size_t)c * M * M);
+      if (l) narrow(lc, l + (size_t)c * M);
       if (info) info[c] = r;
     }
   };
@@ -1236,15 +1414,48 @@ int orc_assemble(void* pp, int C, const double* nodes, const int8_t* parity, con
   return 0;
 }
 
+// Operator rows of one cell (see cell_operators).  With L == NULL only dims
+// {term-component rows, B rows, F rows} are written.  L (QG, rows, N), wm (QG),
+// rterm (rows), U (B rows, M), V (B rows, N), fw (F rows), FV (F rows, N).
+int orc_cell_operators(void* pp, const double* nodes, const int8_t* parity, const double* coeff, int* dims,
+                       double* L, double* wm, int* rterm, double* U, double* V, double* fw, double* FV) {
+  Plan* p = (Plan*)pp;
+  dpg_plan_info pi;
+  orc_plan_query(pp, &pi);
+  size_t cstride = (size_t)p->desc.n_slots * pi.n_points_total;
+  vector<real> xn = widen(nodes, (size_t)p->topo.nv * p->d);
+  vector<real> xc = coeff ? widen(coeff, cstride) : vector<real>();
+  vector<real> L_, wm_, U_, V_, fw_, FV_;
+  vector<int> rt;
+  cell_operators(*p, xn.data(), parity, coeff ? xc.data() : nullptr, L_, wm_, rt, U_, V_, fw_, FV_);
+  dims[0] = (int)rt.size();
+  dims[1] = (int)(U_.size() / p->M);
+  dims[2] = (int)fw_.size();
+  if (!L) return 0;
+  narrow(L_, L); narrow(wm_, wm); narrow(U_, U); narrow(V_, V); narrow(fw_, fw); narrow(FV_, FV);
+  for (size_t i = 0; i < rt.size(); i++) rterm[i] = rt[i];
+  return 0;
+}
+
 // Single-cell factored Cholesky (inputs copied): G row-major NxN, B (M,N), F (N).
 int orc_factored_cholesky_solve(int N, int M, const double* G, const double* B, const double* F, double* K,
                                 double* l) {
-  vector<double> g(G, G + (size_t)N * N), b(B, B + (size_t)M * N), f(F, F + N);
-  return factored_cholesky_solve(N, M, g.data(), b.data(), f.data(), K, l);
+  vector<real> g = widen(G, (size_t)N * N), b = widen(B, (size_t)M * N), f = widen(F, N);
+  vector<real> k((size_t)M * M), ll(M);
+  int r = factored_cholesky_solve(N, M, g.data(), b.data(), f.data(), k.data(), ll.data());
+  narrow(k, K);
+  narrow(ll, l);
+  return r;
 }
 
 int orc_condense(int M, const int* is_field, const double* K, const double* l, double* S, double* s) {
-  return condense(M, is_field, K, l, S, s);
+  int nt = 0;
+  for (int i = 0; i < M; i++) nt += is_field[i] ? 0 : 1;
+  vector<real> k = widen(K, (size_t)M * M), ll = widen(l, M), S_((size_t)nt * nt), s_(nt);
+  int r = condense(M, is_field, k.data(), ll.data(), S_.data(), s_.data());
+  narrow(S_, S);
+  narrow(s_, s);
+  return r;
 }
 
 int orc_trial_is_field(void* pp, int* out) {
@@ -1261,12 +1472,13 @@ int orc_basis_tabulate(int topo, int space, int n, int npts, const double* pts, 
   Basis b = make_basis(topo, space, n);
   if (topo == 0) { b.d = 1; b.card = b.closed.size(); }
   int d = b.d, vdim = b.rank ? d : 1;
-  vector<double> v(b.card * vdim), g(b.card * d), dv(b.card);
+  vector<real> v(b.card * vdim), g(b.card * d), dv(b.card);
   for (int q = 0; q < npts; q++) {
-    b.eval(pts + q * d, v.data(), b.rank ? nullptr : g.data(), b.rank ? dv.data() : nullptr);
-    if (val) std::copy(v.begin(), v.end(), val + (size_t)q * b.card * vdim);
-    if (grad && !b.rank) std::copy(g.begin(), g.end(), grad + (size_t)q * b.card * d);
-    if (div && b.rank) std::copy(dv.begin(), dv.end(), div + (size_t)q * b.card);
+    vector<real> x = widen(pts + q * d, d);
+    b.eval(x.data(), v.data(), b.rank ? nullptr : g.data(), b.rank ? dv.data() : nullptr);
+    if (val) narrow(v, val + (size_t)q * b.card * vdim);
+    if (grad && !b.rank) narrow(g, grad + (size_t)q * b.card * d);
+    if (div && b.rank) narrow(dv, div + (size_t)q * b.card);
   }
   return b.card;
 }
@@ -1274,23 +1486,23 @@ int orc_basis_tabulate(int topo, int space, int n, int npts, const double* pts, 
 // Tensor Gauss rule of a degree on the line (dim 1), quad (2) or hex (3).
 int orc_cubature(int dim, int degree, double* pts, double* wts) {
   Rule r = tensor_gauss(dim, degree);
-  if (pts) std::copy(r.pts.begin(), r.pts.end(), pts);
-  if (wts) std::copy(r.wts.begin(), r.wts.end(), wts);
+  if (pts) narrow(r.pts, pts);
+  if (wts) narrow(r.wts, wts);
   return r.npts();
 }
 
 // Triangle rule exact to `degree` on the reference triangle.
 int orc_tri_cubature(int degree, double* pts, double* wts) {
   Rule r = tri_rule(degree);
-  if (pts) std::copy(r.pts.begin(), r.pts.end(), pts);
-  if (wts) std::copy(r.wts.begin(), r.wts.end(), wts);
+  if (pts) narrow(r.pts, pts);
+  if (wts) narrow(r.wts, wts);
   return r.npts();
 }
 
 // Warp & blend lattice of degree n (the nodes of the triangle HGRAD basis).
 int orc_tri_nodes(int n, double* pts) {
-  vector<double> x = warp_blend_tri(n);
-  if (pts) std::copy(x.begin(), x.end(), pts);
+  vector<real> x = warp_blend_tri(n);
+  if (pts) narrow(x, pts);
   return (int)x.size() / 2;
 }
 

@@ -2,6 +2,11 @@
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py, never by the camellia2_b200 package.
+
+Two builds of the same source: liboracle.so computes in FP64 (the oracle the GPU
+path is compared with); liboracle_xp.so computes in __float128 (`xp=True` below),
+the extended-precision truth for the same double inputs, used to measure how far
+each FP64 code lies from the exact result.
 """
 from __future__ import annotations
 
@@ -14,17 +19,16 @@ import numpy as np
 from camellia2_b200 import abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
 
 
 def build():
     subprocess.check_call(["bash", os.path.join(_HERE, "build.sh")])
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        path = os.path.join(_HERE, "liboracle.so")
+def lib(xp=False):
+    if xp not in _LIBS:
+        path = os.path.join(_HERE, "liboracle_xp.so" if xp else "liboracle.so")
         if not os.path.exists(path):
             build()
         L = ct.CDLL(path)
@@ -40,9 +44,11 @@ def lib():
         L.orc_cubature.argtypes = [ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p]
         L.orc_tri_cubature.argtypes = [ct.c_int, ct.c_void_p, ct.c_void_p]
         L.orc_tri_nodes.argtypes = [ct.c_int, ct.c_void_p]
+        L.orc_cell_operators.argtypes = [ct.c_void_p] * 12
         L.orc_last_error.restype = ct.c_char_p
-        _LIB = L
-    return _LIB
+        assert L.orc_precision() == (1 if xp else 0)
+        _LIBS[xp] = L
+    return _LIBS[xp]
 
 
 def _p(a):
@@ -50,21 +56,25 @@ def _p(a):
 
 
 class OraclePlan:
-    def __init__(self, bucket_or_holder):
+    """One bucket on the CPU.  xp=True computes in __float128 (the truth)."""
+
+    def __init__(self, bucket_or_holder, xp=False):
         holder = getattr(bucket_or_holder, "holder", bucket_or_holder)
         self.holder = holder
-        self.h = lib().orc_plan_create(holder.ptr())
+        self.L = lib(xp)
+        self.xp = xp
+        self.h = self.L.orc_plan_create(holder.ptr())
         if not self.h:
-            raise RuntimeError("oracle plan: " + lib().orc_last_error().decode())
+            raise RuntimeError("oracle plan: " + self.L.orc_last_error().decode())
         info = abi.PlanInfo()
-        lib().orc_plan_query(self.h, ct.byref(info))
+        self.L.orc_plan_query(self.h, ct.byref(info))
         self.info = info.as_dict()
         self.is_field = np.zeros(self.info["M"], dtype=np.int32)
-        lib().orc_trial_is_field(self.h, _p(self.is_field))
+        self.L.orc_trial_is_field(self.h, _p(self.is_field))
 
     def __del__(self):
         try:
-            lib().orc_plan_destroy(self.h)
+            self.L.orc_plan_destroy(self.h)
         except Exception:
             pass
 
@@ -86,9 +96,27 @@ class OraclePlan:
         out["S"] = np.zeros((C, t, t))
         out["s"] = np.zeros((C, t))
         out["info"] = np.zeros(C, dtype=np.int32)
-        lib().orc_assemble(self.h, C, _p(nodes), _p(parity), _p(coeff), _p(out.get("G")), _p(out.get("B")),
+        self.L.orc_assemble(self.h, C, _p(nodes), _p(parity), _p(coeff), _p(out.get("G")), _p(out.get("B")),
                            _p(out.get("F")), _p(out["K"]), _p(out["l"]), _p(out["S"]), _p(out["s"]),
                            _p(out["info"]), nthreads)
+        return out
+
+    def operators(self, nodes, parity, coeff=None):
+        """Quadrature operator rows of ONE cell (nodes (nv, d), parity (ns,), coeff
+        (n_slots, P) or None): G = sum_q wm[q] L[q]^T L[q] (rows = graph-norm term
+        components, rterm their terms), B = U^T V, F = FV^T fw."""
+        i = self.info
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        parity = np.ascontiguousarray(parity, dtype=np.int8)
+        cf = None if coeff is None else np.ascontiguousarray(coeff, dtype=np.float64)
+        dims = np.zeros(3, dtype=np.int32)
+        self.L.orc_cell_operators(self.h, _p(nodes), _p(parity), _p(cf), _p(dims), *([None] * 7))
+        nT, nB, nF = (int(x) for x in dims)
+        N, M, QG = i["N"], i["M"], i["Q_G"]
+        out = dict(L=np.zeros((QG, nT, N)), wm=np.zeros(QG), rterm=np.zeros(nT, dtype=np.int32),
+                   U=np.zeros((nB, M)), V=np.zeros((nB, N)), fw=np.zeros(nF), FV=np.zeros((nF, N)))
+        self.L.orc_cell_operators(self.h, _p(nodes), _p(parity), _p(cf), _p(dims),
+                                  *(_p(out[k]) for k in ("L", "wm", "rterm", "U", "V", "fw", "FV")))
         return out
 
     def parts(self, nodes, parity, coeff=None):
@@ -96,31 +124,31 @@ class OraclePlan:
         C = nodes.shape[0]
         N, M = i["N"], i["M"]
         G, B, F = np.zeros((C, N, N)), np.zeros((C, M, N)), np.zeros((C, N))
-        lib().orc_assemble(self.h, C, _p(np.ascontiguousarray(nodes, dtype=np.float64)),
+        self.L.orc_assemble(self.h, C, _p(np.ascontiguousarray(nodes, dtype=np.float64)),
                            _p(np.ascontiguousarray(parity, dtype=np.int8)),
                            _p(None if coeff is None else np.ascontiguousarray(coeff, dtype=np.float64)),
                            _p(G), _p(B), _p(F), None, None, None, None, None, 1)
         return G, B, F
 
 
-def factored_cholesky_solve(G, B, F):
+def factored_cholesky_solve(G, B, F, xp=False):
     """Single cell: G (N,N), B (M,N) [stiffnessEnriched layout], F (N)."""
     G = np.ascontiguousarray(G, dtype=np.float64)
     B = np.ascontiguousarray(B, dtype=np.float64)
     F = np.ascontiguousarray(F, dtype=np.float64)
     N, M = G.shape[0], B.shape[0]
     K, l = np.zeros((M, M)), np.zeros(M)
-    info = lib().orc_factored_cholesky_solve(N, M, _p(G), _p(B), _p(F), _p(K), _p(l))
+    info = lib(xp).orc_factored_cholesky_solve(N, M, _p(G), _p(B), _p(F), _p(K), _p(l))
     return K, l, info
 
 
-def condense(is_field, K, l):
+def condense(is_field, K, l, xp=False):
     is_field = np.ascontiguousarray(is_field, dtype=np.int32)
     K = np.ascontiguousarray(K, dtype=np.float64)
     l = np.ascontiguousarray(l, dtype=np.float64)
     t = int((is_field == 0).sum())
     S, s = np.zeros((t, t)), np.zeros(t)
-    err = lib().orc_condense(K.shape[0], _p(is_field), _p(K), _p(l), _p(S), _p(s))
+    err = lib(xp).orc_condense(K.shape[0], _p(is_field), _p(K), _p(l), _p(S), _p(s))
     return S, s, err
 
 
