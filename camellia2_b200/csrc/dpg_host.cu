@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <set>
 #include <mutex>
 
 #define DPG_CHA_HOST 4  // points per reverse-mode pull-back chunk (DPG_CHA in the kernel)
@@ -649,7 +650,15 @@ static int smem_layout(DpgPlanDev& g, int chg, bool adj_terms_ok) {
   if ((size_t)g.sm_total * 8 > 232448) {
     return -1;
   }
-  g.scratch_per_cta = (size_t)g.MBT * g.NBT * 64;
+  // Gram sums in two levels: after every 32 points the warps' DMMA accumulators of the
+  // blocks that several graph-norm terms feed are added into FP64 running sums in the
+  // CTA's scratch slot and restart from zero.  A single running sum over all points and
+  // terms puts 1.4x more rounding error into K at h = 1/48 (the reference sums each term
+  // on its own, IP.cpp:238-244); one flush at half way costs ~2 % of the kernel's time,
+  // one every 8 points 17 % (the running sums then cross L2 seven times per cell).
+  g.gflush = std::max(1, 32 / g.chg);
+  g.gsum_off = (size_t)g.MBT * g.NBT * 64;
+  g.scratch_per_cta = g.gsum_off + (size_t)g.ngb * 128;
   return DPG_OK;
 }
 
@@ -939,6 +948,16 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
         for (int e2 = g.rowstart[r]; e2 < g.rowstart[r + 1]; e2++)
           coupled[(g.ipent[e].gslot >> 2) * g.ntest + (g.ipent[e2].gslot >> 2)] = 1;
     std::vector<int> pidx(g.ntest * g.ntest, -1);
+    // var pairs that two or more graph-norm terms couple (their blocks sum products of
+    // very different scales: the ones whose partial sums are flushed)
+    std::vector<std::set<int>> terms_of(g.ntest);
+    for (int e = 0; e < D->n_ip; e++) terms_of[D->ip[e].test_var].insert(D->ip[e].term);
+    auto multi_term = [&](int a, int b) {
+      int n = 0;
+      for (int t : terms_of[a]) n += (int)terms_of[b].count(t);
+      return n >= 2;
+    };
+    std::vector<char> tile_multi;
     int off = 0, np = 0;
     for (int a = 0; a < g.ntest; a++)
       for (int b = 0; b <= a; b++) {
@@ -974,10 +993,21 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
             t.boff = g.hoff[pidx[a * g.ntest + b]] + jj * 8;
             t.ldb = (int16_t)g.test[b].ldA;
             tiles.push_back(t);
+            tile_multi.push_back(multi_term(a, b) ? 1 : 0);
           }
       }
     g.ngb = (int)tiles.size();
     g.ngt = g.NBT * (g.NBT + 1) / 2;
+    {  // the kernel's balanced block ownership: warp w owns blocks [tau0, tau0 + ntw)
+      const int gbase = g.ngb / DPG_NWARPS, gextra = g.ngb % DPG_NWARPS;
+      for (int w = 0; w < DPG_NWARPS; w++) {
+        const int ntw = gbase + (w < gextra ? 1 : 0), tau0 = w * gbase + std::min(w, gextra);
+        uint32_t bits = 0;
+        for (int u = 0; u < ntw && u < 32; u++)
+          if (tile_multi[tau0 + u]) bits |= 1u << u;
+        g.gflushbits[w] = bits;
+      }
+    }
     std::vector<int> gz;  // lower tiles no block writes (uncoupled var pairs)
     for (int u = 0; u < g.ngt && !g.big; u++)
       if (!covered[u]) gz.push_back(u);

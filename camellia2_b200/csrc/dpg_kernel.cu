@@ -609,9 +609,14 @@ __device__ __noinline__ void phase_b(const DpgPlanDev& P, const DpgLaunch& L, in
 
 // The Gram chunk loop for CH points per chunk (compile-time, so the h and DMMA loops
 // unroll completely).
+// Every P.gflush chunks (except after the last) each thread adds the accumulators of its
+// flushed blocks (P.gflushbits) into its own running sums in gsum ([block][lane][4]; plain
+// L2 loads and stores, one writer per element, so the order of additions is fixed) and
+// restarts them from zero.
 template <int GTM, int CH>
 __device__ __forceinline__ void gram_chunks(const DpgPlanDev& P, const Ctx& X, const double* Dm, double* hb, int nunit,
-                                            int ntw, const uint32_t (&pk)[GTM], double (&acc)[GTM][4]) {
+                                            int ntw, const uint32_t (&pk)[GTM], double (&acc)[GTM][4],
+                                            double* __restrict__ gsum) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   DPG_SMEM_VIEWS(P);
@@ -673,6 +678,24 @@ __device__ __forceinline__ void gram_chunks(const DpgPlanDev& P, const Ctx& X, c
 #pragma unroll
           for (int i = 0; i < 4; i++) bv[i] = hq[i * P.hstride + bo];
           dmma16(acc[u], av, bv);
+        }
+      }
+    }
+    if (P.gflush > 0 && (c + 1) % P.gflush == 0 && c + 1 < nch) {
+      const bool first = (c + 1) == P.gflush;
+      const uint32_t fb = P.gflushbits[warp];
+#pragma unroll
+      for (int u = 0; u < GTM; u++) {
+        if (u < ntw && ((fb >> u) & 1u)) {
+          double2* sp = reinterpret_cast<double2*>(gsum + (u * 32 + lane) * 4);
+          double2 lo = make_double2(acc[u][0], acc[u][1]), hi = make_double2(acc[u][2], acc[u][3]);
+          if (!first) {
+            const double2 a = __ldcg(sp), b = __ldcg(sp + 1);
+            lo.x = a.x + lo.x; lo.y = a.y + lo.y; hi.x = b.x + hi.x; hi.y = b.y + hi.y;
+          }
+          __stcg(sp, lo);
+          __stcg(sp + 1, hi);
+          acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
         }
       }
     }
@@ -759,9 +782,22 @@ __device__ __forceinline__ void phase_gram(const DpgPlanDev& P, const DpgLaunch&
   int nunit = 0;
   for (int p = 0; p < P.npairs; p++) nunit += P.test[P.pair_b[p]].ntiles;
   __syncthreads();
-  if (CHG != 0) gram_chunks<GTM, CHG != 0 ? CHG : DPG_CHG>(P, X, Dm, hb, nunit, ntw, pk, acc);
-  else if (P.chg == DPG_CHG) gram_chunks<GTM, DPG_CHG>(P, X, Dm, hb, nunit, ntw, pk, acc);
-  else gram_chunks<GTM, DPG_CHG / 2>(P, X, Dm, hb, nunit, ntw, pk, acc);
+  double* gsum = L.scratch + (size_t)blockIdx.x * P.scratch_per_cta + P.gsum_off + (size_t)tau0 * 128;
+  if (CHG != 0) gram_chunks<GTM, CHG != 0 ? CHG : DPG_CHG>(P, X, Dm, hb, nunit, ntw, pk, acc, gsum);
+  else if (P.chg == DPG_CHG) gram_chunks<GTM, DPG_CHG>(P, X, Dm, hb, nunit, ntw, pk, acc, gsum);
+  else gram_chunks<GTM, DPG_CHG / 2>(P, X, Dm, hb, nunit, ntw, pk, acc, gsum);
+  if (P.gflush > 0 && P.gflush < P.QGpad / P.chg) {  // the last group joins the running sums
+    const uint32_t fb = P.gflushbits[warp];
+#pragma unroll
+    for (int u = 0; u < GTM; u++) {
+      if (u < ntw && ((fb >> u) & 1u)) {
+        const double2* sp = reinterpret_cast<const double2*>(gsum + (u * 32 + lane) * 4);
+        const double2 a = __ldcg(sp), b = __ldcg(sp + 1);
+        acc[u][0] = a.x + acc[u][0]; acc[u][1] = a.y + acc[u][1];
+        acc[u][2] = b.x + acc[u][2]; acc[u][3] = b.y + acc[u][3];
+      }
+    }
+  }
   // accumulators -> tile-lower shared storage (overlaps the staging area); tiles of
   // uncoupled var pairs are zero
   for (int e = tid; e < P.ngz * 64; e += NT) GT[P.gzero[e >> 6] * 64 + (e & 63)] = 0.0;

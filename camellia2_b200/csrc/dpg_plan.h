@@ -193,7 +193,14 @@ struct DpgPlanDev {
   int sm_w, sm_k;                                  // solve / Gram of W
   int a_sa, a_ldS;                                 // adjoint: S_A [MBT*8][a_ldS]
   int a_fs, a_xpf, a_ldx, a_geo, a_beta, a_cbar;   // adjoint pull-back
-  size_t scratch_per_cta;                          // doubles of B scratch per CTA
+  size_t scratch_per_cta;                          // doubles of scratch per CTA: B tiles, then
+                                                   // the Gram running sums at gsum_off
+  size_t gsum_off;                                 // [ngb][32 lanes][4] Gram partial sums
+  int gflush;                                      // staged Gram chunks between two flushes of the
+                                                   // accumulators into the running sums (0: none)
+  uint32_t gflushbits[DPG_NWARPS];                 // per warp: its blocks (bit u = its u-th) that
+                                                   // take part in the flushes (var pairs that two
+                                                   // or more graph-norm terms couple)
   // Large buckets (N > 192 or M > 120 after padding) run on dpg_big_kernel: per cell the
   // lower triangle of Z = [[G, E], [E^T, 0]] (E = [B^T | F]; rows/columns: device test rows,
   // then device trial columns) in a per-CTA global workspace.

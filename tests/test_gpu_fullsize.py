@@ -8,8 +8,9 @@ sample of cells spread over the whole mesh:
     same cells of the full launch (no cross-cell state in the persistent kernel);
   - on the sampled cells the quadrature products G, B, F match the oracle to 1e-13
     (their accuracy does not depend on h), and K, l, S, s to 1e-12 or, where the
-    cell's Gram conditioning sets a higher FP64 floor (h = 1/48: cond(G) ~ 1e14), to
-    10x the change of K under 1-ulp perturbations of G.
+    cell's Gram conditioning puts two FP64 codes further apart (h = 1/48: cond(G) ~ 1e14),
+    the GPU's error against the extended-precision truth is at most three times the FP64
+    oracle's own.
 
 The symmetry reductions run on the device in slices of cells, so no output leaves the
 GPU except the sampled cells."""
@@ -20,7 +21,7 @@ torch = pytest.importorskip("torch")
 
 from camellia2_b200 import abi, formulation as fm, lib as dlib, mesh  # noqa: E402
 from tests.conftest import rel_fro  # noqa: E402
-from tests.test_gpu_parity import fp64_floor  # noqa: E402
+from tests.helpers import check_against_truth  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -86,11 +87,4 @@ def test_full_size_properties(make, oracle_mod):
         assert rel_fro(G[j], ref["G"][j]) < 1e-13
         assert rel_fro(B[j], ref["B"][j]) < 1e-13
         assert rel_fro(F[j], ref["F"][j]) < 1e-13
-        errs = {k: rel_fro(got[k][j], ref[k][j]) for k in got}
-        tol = 1e-12
-        if max(errs.values()) >= tol:
-            floor = fp64_floor(oracle_mod, ref["G"][j], ref["B"][j], ref["F"][j], ref["K"][j])
-            if floor > 2e-13:
-                tol = 10 * floor
-        for k, e in errs.items():
-            assert e < tol, (int(pick[j]), k, e, tol)
+    check_against_truth(oracle_mod, bucket, nodes[pick], par[pick], None if co is None else co[pick], got, ref)

@@ -104,7 +104,7 @@ def test_triangle_rt_basis_is_well_conditioned(oracle_mod, p):
     the finest cells of the uneven-cell workload (h = 1/256), where every factorisation
     succeeds.  With x times monomials the floor was 1.4e-8 at h = 1 and the Gram matrix lost
     positive definiteness at h = 1/256 for p = 6."""
-    from tests.test_gpu_parity import fp64_floor
+    from tests.helpers import fp64_floor
     b = fm.StokesVGPFormulation(2).bucket(abi.TOPO_TRI, p, 2)
     P = oracle_mod.OraclePlan(b)
     for base_n, bound in ((1, 1e-11), (256, 1e-6)):
