@@ -517,27 +517,21 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
       // G (N, N), B (M, N) and F (N) in user numbering: Z unscaled (dpg_assemble_parts)
       __syncthreads();
       const int N = P.N;
-      auto dev_test = [&](int u) {
-        int dv = 0;
-        for (int a = 0; a < P.ntest; a++)
-          if (u >= P.test[a].user_off && u < P.test[a].user_off + P.test[a].card) dv = P.test[a].dev_off + u - P.test[a].user_off;
-        return dv;
-      };
       if (L.G)
-        for (size_t e = tid; e < (size_t)N * N; e += NT) {
-          const int ur = (int)(e / N), uc = (int)(e - (size_t)ur * N);
-          const int dr = dev_test(ur), dc = dev_test(uc);
+        for (int e = tid; e < N * N; e += NT) {
+          const int ur = e / N, uc = e - ur * N;
+          const int dr = __ldg(P.u2d_test + ur), dc = __ldg(P.u2d_test + uc);
           L.G[(size_t)cell * N * N + e] = Z[(size_t)max(dr, dc) * ld + min(dr, dc)] / (S.sc[dr] * S.sc[dc]);
         }
       if (L.B)
-        for (size_t e = tid; e < (size_t)M * N; e += NT) {
-          const int ut = (int)(e / N), us = (int)(e - (size_t)ut * N);
-          const int ds = dev_test(us);
+        for (int e = tid; e < M * N; e += NT) {
+          const int ut = e / N, us = e - ut * N;
+          const int ds = __ldg(P.u2d_test + us);
           L.B[(size_t)cell * M * N + e] = Z[(size_t)(Np + __ldg(P.u2d_trial + ut)) * ld + ds] / S.sc[ds];
         }
       if (L.F)
         for (int us = tid; us < N; us += NT) {
-          const int ds = dev_test(us);
+          const int ds = __ldg(P.u2d_test + us);
           L.F[(size_t)cell * N + us] = Z[(size_t)(Np + P.fcol) * ld + ds] / S.sc[ds];
         }
       __syncthreads();
@@ -561,7 +555,8 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
       if (tid == 0) {
         double e2 = 0.0;
         for (int w = 0; w < NT / 32; w++) e2 += red[w];
-        L.energy[cell] = sqrt(e2);
+        // a failed factorisation of the test block leaves no energy to report
+        L.energy[cell] = S.ints[0] == BIG_NOFAIL ? sqrt(e2) : __longlong_as_double(0x7ff8000000000000ll);
       }
     } else {
     // trailing block = -[K_ext]: K, l out, then negate (padded field columns get a unit pivot)

@@ -61,13 +61,14 @@ __global__ void __launch_bounds__(NT, 1) dpg_energy_kernel(const __grid_constant
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
       if (lane == 0) {
-        L.energy[cell] = sqrt(acc);
         int v = 0;
         if (flag_s[2]) v = ERR_TIMEOUT_FLAG;
         else if (flag_s[0] != 0) {
           const int r = flag_s[0] - 1, u = P.dev2user_test[r];
           v = (u >= 0 ? u : r) + 1;
         }
+        // a failed factorisation leaves no energy to report
+        L.energy[cell] = v == 0 ? sqrt(acc) : __longlong_as_double(0x7ff8000000000000ll);
         if (L.info) L.info[cell] = v;
       }
     }

@@ -572,6 +572,10 @@ static int big_layout(HostPlan* P) {
     for (int i = 0; i < cnt; i++) u2d[tr.user_off + i] = tr.dev_off + i;
   }
   g.u2d_trial = upload_i(P, u2d);
+  std::vector<int> u2dt(g.N, 0);
+  for (int a = 0; a < g.ntest; a++)
+    for (int i = 0; i < g.test[a].card; i++) u2dt[g.test[a].user_off + i] = g.test[a].dev_off + i;
+  g.u2d_test = upload_i(P, u2dt);
   auto al = [](size_t x) { return (x + 31) & ~(size_t)31; };  // 256-byte aligned regions
   size_t o = al((size_t)g.Zn * g.ldz);
   g.bz_wq = (int)o; o += al(g.QGpad);
@@ -667,6 +671,13 @@ static int build(HostPlan* P, const dpg_bucket_desc* D) {
   std::memset(&g, 0, sizeof(g));
   TopoData T;
   if (!topo_data(D->topology, T)) return fail(DPG_ERR_INVALID_ARGUMENT, "unknown topology");
+  // Only the FP64 form is built.  The split-precision recipes with FP32 accumulation
+  // (3-term BF16 or TF32) leave the condensed matrix 1e-3..1 away from the FP64 result at
+  // h = 1/48, and the integer-slicing recipe that reaches 1e-10 (six int8 slices, 36 exact
+  // slice products) replaces only the Gram quadrature, a third of the kernel's time.
+  if (D->precision == DPG_PREC_MIXED)
+    return fail(DPG_ERR_UNSUPPORTED, "DPG_PREC_MIXED: no mixed-precision form is built; use DPG_PREC_FP64");
+  if (D->precision != DPG_PREC_FP64) return fail(DPG_ERR_INVALID_ARGUMENT, "unknown precision mode");
   const int topo = D->topology;
   if (D->n_test < 1 || D->n_test > DPG_MAXV || D->n_trial < 1 || D->n_trial > DPG_MAXV)
     return fail(DPG_ERR_UNSUPPORTED, "number of test/trial vars out of range (1..16)");
@@ -1595,7 +1606,7 @@ int dpg_plan_autotune(dpg_plan* p, int C, const double* nodes, const int8_t* par
   const DpgPlanDev& g0 = p->hp.dev;
   const size_t nK = (size_t)C * g0.M * g0.M, nl = (size_t)C * g0.M, nS = (size_t)C * g0.nt * g0.nt, ns = (size_t)C * g0.nt;
   void* out = nullptr;
-  if (cudaMallocAsync(&out, (nK + nl + nS + ns) * sizeof(double) + (size_t)C * 4, st) != cudaSuccess) {
+  if (dpg::ws_alloc(&out, (nK + nl + nS + ns) * sizeof(double) + (size_t)C * 4, st) != cudaSuccess) {
     cudaGetLastError();
     return fail(DPG_ERR_OUT_OF_MEMORY, "autotune outputs");
   }

@@ -9,6 +9,14 @@
 namespace dpg {
 extern thread_local std::string g_last_error;
 int fail(int code, const std::string& msg);
+// Stream-ordered workspace allocation.  Outside stream capture it draws from a memory
+// pool the library owns on the current device (created on first use, with a release
+// threshold that keeps freed workspaces between calls); the caller's pools and the
+// device's default pool are not modified.  Inside a capture it uses cudaMallocAsync,
+// which the capture turns into a graph allocation.  Free with cudaFreeAsync.
+cudaError_t ws_alloc(void** p, size_t bytes, cudaStream_t s);
+// Number of SMs of the current device (cached per device).
+int num_sms();
 }  // namespace dpg
 
 // Arguments of one assembly launch (device pointers).

@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 // The CTA's dynamic shared memory; every shared pointer below is derived from it
@@ -1257,9 +1258,63 @@ static MultiFn pick_multi_kernel(const DpgPlanDev* plans, int nb) {
   return nullptr;
 }
 
-static int g_num_sms = 0;
-
 }  // namespace
+
+namespace dpg {
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_dev_mu;
+int g_dev_sms[kMaxDevices] = {0};
+cudaMemPool_t g_dev_pool[kMaxDevices] = {nullptr};
+bool g_dev_pool_tried[kMaxDevices] = {false};
+}  // namespace
+
+int num_sms() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= kMaxDevices) return 148;
+  std::lock_guard<std::mutex> g(g_dev_mu);
+  if (g_dev_sms[dev] == 0) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    g_dev_sms[dev] = n > 0 ? n : 1;
+    cudaGetLastError();
+  }
+  return g_dev_sms[dev];
+}
+
+cudaError_t ws_alloc(void** p, size_t bytes, cudaStream_t s) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusNone;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaMemPool_t pool = nullptr;
+  if (cap == cudaStreamCaptureStatusNone && dev >= 0 && dev < kMaxDevices) {
+    std::lock_guard<std::mutex> g(g_dev_mu);
+    if (!g_dev_pool_tried[dev]) {
+      g_dev_pool_tried[dev] = true;
+      cudaMemPoolProps props;
+      std::memset(&props, 0, sizeof(props));
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaMemPool_t created = nullptr;
+      if (cudaMemPoolCreate(&created, &props) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &thr);
+        g_dev_pool[dev] = created;
+      }
+      cudaGetLastError();
+    }
+    pool = g_dev_pool[dev];
+  }
+  if (pool) return cudaMallocFromPoolAsync(p, bytes, pool, s);
+  return cudaMallocAsync(p, bytes, s);
+}
+}  // namespace dpg
 
 static int configure_big(const DpgPlanDev* plan) {
   int dev = 0, optin = 0;
@@ -1272,17 +1327,6 @@ static int configure_big(const DpgPlanDev* plan) {
   if (optin > 0) bytes = (size_t)optin;
   cudaError_t e = cudaFuncSetAttribute(dpg_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-  if (g_num_sms == 0) {
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 1;
-    // keep freed stream-ordered workspaces in the pool between calls
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      uint64_t thr = UINT64_MAX;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
-    cudaGetLastError();
-  }
   return DPG_OK;
 }
 
@@ -1290,11 +1334,11 @@ static int configure_big(const DpgPlanDev* plan) {
 static int launch_big(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
   if (Lin->solve_only)
     return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans support the assembly entry points only");
-  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  const int grid = std::min(Lin->C, dpg::num_sms());
   DpgLaunch L = *Lin;
   void* ws = nullptr;
   if (!L.scratch) {  // a caller-provided workspace holds dpg_big_workspace_bytes(plan, C)
-    cudaError_t ea = cudaMallocAsync(&ws, (size_t)grid * plan->bz_per_cta * sizeof(double), stream);
+    cudaError_t ea = dpg::ws_alloc(&ws, (size_t)grid * plan->bz_per_cta * sizeof(double), stream);
     if (ea != cudaSuccess) {
       cudaGetLastError();
       return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("workspace allocation: ") + cudaGetErrorString(ea));
@@ -1309,7 +1353,7 @@ static int launch_big(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t
 }
 
 size_t dpg_big_workspace_bytes(const DpgPlanDev* plan, int C) {
-  const int grid = std::min(std::max(C, 1), g_num_sms > 0 ? g_num_sms : 148);
+  const int grid = std::min(std::max(C, 1), dpg::num_sms());
   return (size_t)grid * plan->bz_per_cta * sizeof(double);
 }
 
@@ -1335,17 +1379,6 @@ int dpg_configure_kernels(const DpgPlanDev* plan) {
         return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     }
   }
-  if (g_num_sms == 0) {
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 1;
-    // keep freed stream-ordered scratch in the pool between calls
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      uint64_t thr = UINT64_MAX;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
-    cudaGetLastError();
-  }
   return DPG_OK;
 }
 
@@ -1355,12 +1388,12 @@ int dpg_launch_assemble(const DpgPlanDev* plan, const DpgPlanDev* d_plan, const 
   if (plan->big) return launch_big(plan, Lin, stream);
   KernelFn k = pick_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
-  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  const int grid = std::min(Lin->C, dpg::num_sms());
   DpgLaunch L = *Lin;
   void* scratch = nullptr;
   const bool need_scratch = !L.solve_only && plan->scratch_per_cta > 0 && !L.scratch;
   if (need_scratch) {
-    cudaError_t ea = cudaMallocAsync(&scratch, (size_t)grid * plan->scratch_per_cta * sizeof(double), stream);
+    cudaError_t ea = dpg::ws_alloc(&scratch, (size_t)grid * plan->scratch_per_cta * sizeof(double), stream);
     if (ea != cudaSuccess) {
       cudaGetLastError();
       return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(ea));
@@ -1592,7 +1625,7 @@ int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const doubl
     }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, recover_fields_warp_kernel, 32, per_warp);
-    const int sms = g_num_sms > 0 ? g_num_sms : 148;
+    const int sms = dpg::num_sms();
     const int grid = (int)std::min<long long>(C, (long long)sms * std::max(1, per_sm));
     recover_fields_warp_kernel<<<grid, 32, per_warp, stream>>>(C, M, nf, K, l, t, u, info);
     cudaError_t e = cudaGetLastError();
@@ -1606,7 +1639,7 @@ int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const doubl
     cudaFuncSetAttribute(recover_fields_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     configured = 1;
   }
-  const int grid = std::min(C, (g_num_sms > 0 ? g_num_sms : 148) * 4);
+  const int grid = std::min(C, (dpg::num_sms()) * 4);
   recover_fields_kernel<<<grid, 256, bytes, stream>>>(C, M, nf, K, l, t, u, info);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
@@ -1642,11 +1675,11 @@ int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_
   if (!plan->adj_ok) return dpg::fail(DPG_ERR_UNSUPPORTED, "reverse mode is not available for this bucket");
   KernelFn k = pick_adjoint_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no adjoint kernel instance for this bucket size");
-  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  const int grid = std::min(Lin->C, dpg::num_sms());
   DpgLaunch L = *Lin;
   void* scratch = nullptr;
   const size_t per = plan->scratch_per_cta;
-  cudaError_t ea = cudaMallocAsync(&scratch, (size_t)grid * per * 2 * sizeof(double), stream);
+  cudaError_t ea = dpg::ws_alloc(&scratch, (size_t)grid * per * 2 * sizeof(double), stream);
   if (ea != cudaSuccess) {
     cudaGetLastError();
     return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(ea));
@@ -1675,10 +1708,10 @@ int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        optin > 0 ? optin : (int)(plan->sm_total * sizeof(double)));
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-  const int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  const int grid = std::min(Lin->C, dpg::num_sms());
   DpgLaunch L = *Lin;
   void* scratch = nullptr;
-  cudaError_t ea = cudaMallocAsync(&scratch, (size_t)grid * plan->scratch_per_cta * sizeof(double), stream);
+  cudaError_t ea = dpg::ws_alloc(&scratch, (size_t)grid * plan->scratch_per_cta * sizeof(double), stream);
   if (ea != cudaSuccess) {
     cudaGetLastError();
     return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(ea));
@@ -1716,7 +1749,7 @@ int dpg_launch_multi(const DpgPlanDev* hplans_in, const DpgLaunch* hl_in, int nb
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev_id);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin > 0 ? optin : (int)smem);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-  const int grid = std::min(total, g_num_sms > 0 ? g_num_sms : 148);
+  const int grid = std::min(total, dpg::num_sms());
   for (auto& p : hplans) p.scratch_per_cta = stride;
   const size_t bytes_tables = nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)) + (nb + 1) * sizeof(int) + 256;
   const size_t bytes_scratch = (size_t)grid * stride * sizeof(double);
@@ -1725,7 +1758,7 @@ int dpg_launch_multi(const DpgPlanDev* hplans_in, const DpgLaunch* hl_in, int nb
     if (dev->bytes < bytes_tables + bytes_scratch) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "multi workspace too small");
     base = (char*)dev->base;
   } else {
-    e = cudaMallocAsync((void**)&base, bytes_tables + bytes_scratch, stream);
+    e = dpg::ws_alloc((void**)&base, bytes_tables + bytes_scratch, stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("multi workspace: ") + cudaGetErrorString(e));
@@ -1771,26 +1804,52 @@ size_t dpg_multi_bytes(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb) {
     stride = std::max(stride, hplans[b].scratch_per_cta);
     total += std::max(0, hl[b].C);
   }
-  const int grid = std::min(std::max(total, 1), g_num_sms > 0 ? g_num_sms : 148);
+  const int grid = std::min(std::max(total, 1), dpg::num_sms());
   const size_t tables = nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)) + (nb + 1) * sizeof(int) + 256;
   return ((tables + 255) & ~(size_t)255) + (size_t)grid * stride * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
 // Allocation-free launch: the per-CTA scratch comes from a fixed device array
-// instead of a stream-ordered allocation.  32 MiB (4 Mi doubles) is enough for
-// one CTA per SM at the largest buckets of the single-CTA kernel that fit in it
-// (the 3D hex k=2 bucket needs 165 KiB per CTA).
+// instead of a stream-ordered allocation.  32 MiB (4 Mi doubles): the 3D hex k=2
+// bucket needs 298 KiB per CTA (B tiles 165 KiB, Gram running sums 133 KiB), so
+// 110 CTAs fit; smaller buckets run one CTA per SM.
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 #define DPG_NOALLOC_SCRATCH_DOUBLES ((size_t)4 << 20)
 
 static __device__ __align__(256) double g_noalloc_scratch[DPG_NOALLOC_SCRATCH_DOUBLES];
 
 namespace {
 std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[64] = {nullptr};  // device address of the array, per device ordinal
+double* g_noalloc_ptr[64] = {nullptr};           // device address of the array, per device ordinal
+unsigned long long g_noalloc_ctx[64] = {0};      // id of the context that address belongs to
+
+// Id of the current CUDA context (0 if the driver cannot tell).  A device reset
+// followed by a new context changes it, and the array's address must then be looked
+// up again.  The driver functions are reached through the runtime's entry-point query,
+// so the library needs no link against the driver library.
+unsigned long long current_context_id() {
+  typedef int (*CtxGetCurrent)(void**);
+  typedef int (*CtxGetId)(void*, unsigned long long*);
+  static CtxGetCurrent get_current = nullptr;
+  static CtxGetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {  // called with g_noalloc_mu held
+    looked_up = true;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+    cudaGetLastError();
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+  return 0;
+}
 }  // namespace
 
 int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
@@ -1809,7 +1868,8 @@ int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* Lin, cu
   double* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_noalloc_ptr[dev] || (ctx != 0 && ctx != g_noalloc_ctx[dev])) {
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
@@ -1818,11 +1878,12 @@ int dpg_launch_assemble_noalloc(const DpgPlanDev* plan, const DpgLaunch* Lin, cu
                                            cudaGetErrorString(e));
       }
       g_noalloc_ptr[dev] = (double*)p;
+      g_noalloc_ctx[dev] = current_context_id();  // the lookup made the context current if none was
     }
     base = g_noalloc_ptr[dev];
   }
   const size_t fit = plan->scratch_per_cta > 0 ? DPG_NOALLOC_SCRATCH_DOUBLES / plan->scratch_per_cta : (size_t)Lin->C;
-  int grid = std::min(Lin->C, g_num_sms > 0 ? g_num_sms : 148);
+  int grid = std::min(Lin->C, dpg::num_sms());
   grid = (int)std::min<size_t>((size_t)grid, fit);
   DpgLaunch L = *Lin;
   L.scratch = base;

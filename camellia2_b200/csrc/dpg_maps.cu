@@ -101,7 +101,7 @@ int inclusive_scan(int64_t* x, long long n, cudaStream_t st) {
     return DPG_OK;
   }
   int64_t* sums = nullptr;
-  if (cudaMallocAsync((void**)&sums, (size_t)nb * sizeof(int64_t), st) != cudaSuccess) {
+  if (dpg::ws_alloc((void**)&sums, (size_t)nb * sizeof(int64_t), st) != cudaSuccess) {
     cudaGetLastError();
     return dpg::fail(DPG_ERR_OUT_OF_MEMORY, "scan workspace allocation failed");
   }
@@ -584,7 +584,7 @@ extern "C" int dpg_scatter_plan_create(int C, int t, const int64_t* map_ptr, con
   // the largest number of map entries of a cell sizes the shared tables
   void* tmp = nullptr;
   const size_t cnt_bytes = 3 * ((size_t)C + 1) * sizeof(int64_t);
-  if (cudaMallocAsync(&tmp, cnt_bytes + 16, st) != cudaSuccess) {
+  if (dpg::ws_alloc(&tmp, cnt_bytes + 16, st) != cudaSuccess) {
     cudaGetLastError();
     delete P;
     return dpg::fail(DPG_ERR_OUT_OF_MEMORY, "scatter plan workspace allocation failed");

@@ -210,6 +210,7 @@ struct DpgPlanDev {
   int4 be[DPG_MAX_BF];      // (segment, segment-local term, first vt row, points)
   int ipmask[DPG_MAX_IPROWS];  // test vars each IP row touches (bit a)
   const int* u2d_trial;     // [M] user trial index -> device column
+  const int* u2d_test;      // [N] user test index -> device row
   int bz_wq, bz_bh, bz_vt;  // per-CTA workspace after Z: w|J| at Gram points, per-point IP row
                             // factors [QG][rows][ntest][4], per-point term factors [vt rows][4]
   size_t bz_per_cta;        // doubles of per-CTA workspace

@@ -103,9 +103,12 @@ extern "C" {
 #define DPG_OP_DIV 7
 #define DPG_OP_DOT_NORMAL 8 /* tau . n on a side */
 
-/* precision of the quadrature contractions */
+/* precision of the quadrature contractions.  Only DPG_PREC_FP64 is built:
+ * dpg_plan_create returns DPG_ERR_UNSUPPORTED for DPG_PREC_MIXED (split-precision
+ * tensor-core contractions with an FP64 factor/solve), whose accuracy at the target
+ * meshes is below the bar for the recipes with FP32 accumulation. */
 #define DPG_PREC_FP64 0
-#define DPG_PREC_MIXED 1 /* split-precision tensor-core contractions, FP64 factor/solve */
+#define DPG_PREC_MIXED 1
 
 /* dpg_assemble flags */
 #define DPG_FLAG_NO_K 1        /* do not write K / l (condensed outputs only) */
@@ -270,7 +273,8 @@ int dpg_assemble_dls(dpg_plan* plan, int C, const double* nodes, const int8_t* p
  * with computeErrorRepresentation (src/Solution/Solution.cpp:2653-2722).  For the
  * cells' local trial coefficients x (C,M; user numbering, fields first) writes
  * energy[c] = sqrt(r^T G^-1 r), r = F - B x the residual on the test space.
- * info as for dpg_assemble.  Device pointers. */
+ * info as for dpg_assemble; a cell whose Gram factorisation fails (info != 0)
+ * gets energy[c] = NaN.  Device pointers. */
 int dpg_energy_error(dpg_plan* plan, int C, const double* nodes, const int8_t* parity, const double* coeff,
                      const double* local_coeff, double* energy, int32_t* info, void* stream);
 
@@ -369,16 +373,19 @@ int dpg_graph_destroy(dpg_graph* graph);
  * several solver ranks), or a time-stepping loop that must not take allocation
  * latency or an out-of-memory failure in the middle of a step.
  * dpg_assemble takes its per-CTA scratch (the B tiles held between the B phase
- * and the triangular solve) from a stream-ordered allocation; this variant
- * uses a fixed 32 MiB array that the library reserves on every GPU that loads
- * it, until the process exits.  Same arguments, outputs and errors as
- * dpg_assemble, plus:
+ * and the triangular solve, and the Gram matrix's running sums) from a
+ * stream-ordered allocation; this variant uses a fixed 32 MiB array that the
+ * library reserves on every GPU that loads it, until the process exits.  Same
+ * arguments, outputs and errors as dpg_assemble, plus:
  *   - the first call on a device looks the array up (cudaGetSymbolAddress) with
- *     that device current; make that first call before any stream capture;
- *   - buckets whose per-CTA scratch exceeds 32 MiB are rejected with
- *     DPG_ERR_UNSUPPORTED; otherwise the launch uses as many CTAs as fit
- *     (floor(32 MiB / per-CTA scratch), at most one per SM), so large buckets
- *     run on fewer SMs;
+ *     that device current, and so does the first call after that device's
+ *     context was destroyed and recreated (cudaDeviceReset); make those calls
+ *     outside any stream capture;
+ *   - large-bucket plans (more than 192 test rows or 120 trial columns after
+ *     padding) are rejected with DPG_ERR_UNSUPPORTED, and so are buckets whose
+ *     per-CTA scratch exceeds 32 MiB; otherwise the launch uses as many CTAs as
+ *     fit (floor(32 MiB / per-CTA scratch), at most one per SM): the 3D hex k=2
+ *     bucket (298 KiB per CTA) runs on 110 CTAs;
  *   - every call shares the one array: calls that overlap on the GPU (other
  *     streams, other threads, other plans) race and must be serialised by the
  *     caller.  The array keeps the last call's contents; every call writes the

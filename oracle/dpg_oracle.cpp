@@ -1127,6 +1127,181 @@ static void cell_operators(const Plan& P, const real* nodes, const int8_t* parit
     }
 }
 
+// Reverse mode (no counterpart in the reference; the hand gradient that the GPU's
+// dpg_assemble_adjoint is checked against).  For J = <Kbar, K> + <lbar, l> on one cell,
+// with X = G^-1 B^T and y = G^-1 F (B stored trial x test, K = B G^-1 B^T, l = B G^-1 F):
+//   Bbar = (Kbar + Kbar^T) X^T + lbar y^T,   Fbar = X lbar,
+//   Gbar + Gbar^T = -(X (Kbar + Kbar^T) X^T + X lbar y^T + y lbar^T X^T),
+// then dJ/dslot(p) = <Bbar, dB/dslot(p)> + <Gbar, dG/dslot(p)> + Fbar . dF/dslot(p) through
+// the same quadrature as assemble_cell (every form is linear in each coefficient slot
+// value of a term, the Gram matrix quadratic through its rows L_r).
+static void adjoint_cell(const Plan& P, const real* nodes, const int8_t* parity, const real* coeff,
+                         const real* Kbar, const real* lbar, real* cbar) {
+  const int N = P.N, M = P.M, d = P.d;
+  const int QG = P.rG.npts(), QB = P.rB.npts(), QS = P.rS.npts();
+  const int Ptot = QG + QB + P.topo.nsides * QS;
+  CellOut o;
+  assemble_cell(P, nodes, parity, coeff, o);
+  // Cholesky of the equilibrated G (as BF.cpp:944-982), then X = G^-1 B^T and y = G^-1 F
+  vector<real> s(N), Lf((size_t)N * N, 0.0);
+  for (int i = 0; i < N; i++) s[i] = 1.0 / r_sqrt(o.G[(size_t)i * N + i]);
+  for (int j = 0; j < N; j++) {
+    real ajj = o.G[(size_t)j * N + j] * s[j] * s[j];
+    for (int k = 0; k < j; k++) ajj -= Lf[(size_t)j * N + k] * Lf[(size_t)j * N + k];
+    ajj = r_sqrt(ajj);
+    Lf[(size_t)j * N + j] = ajj;
+    for (int i = j + 1; i < N; i++) {
+      real v = o.G[(size_t)i * N + j] * s[i] * s[j];
+      for (int k = 0; k < j; k++) v -= Lf[(size_t)i * N + k] * Lf[(size_t)j * N + k];
+      Lf[(size_t)i * N + j] = v / ajj;
+    }
+  }
+  auto solve = [&](real* b) {  // b <- G^-1 b = S (Ls Ls^T)^-1 S b
+    for (int i = 0; i < N; i++) b[i] *= s[i];
+    for (int i = 0; i < N; i++) {
+      real v = b[i];
+      for (int k = 0; k < i; k++) v -= Lf[(size_t)i * N + k] * b[k];
+      b[i] = v / Lf[(size_t)i * N + i];
+    }
+    for (int i = N - 1; i >= 0; i--) {
+      real v = b[i];
+      for (int k = i + 1; k < N; k++) v -= Lf[(size_t)k * N + i] * b[k];
+      b[i] = v / Lf[(size_t)i * N + i];
+    }
+    for (int i = 0; i < N; i++) b[i] *= s[i];
+  };
+  vector<real> X((size_t)M * N), y(o.F);  // X stored as rows m: (G^-1 B^T)[:, m]
+  for (int m = 0; m < M; m++) {
+    std::copy(&o.B[(size_t)m * N], &o.B[(size_t)m * N] + N, &X[(size_t)m * N]);
+    solve(&X[(size_t)m * N]);
+  }
+  solve(y.data());
+  vector<real> Ks((size_t)M * M);
+  for (int a = 0; a < M; a++)
+    for (int b = 0; b < M; b++) Ks[(size_t)a * M + b] = Kbar[(size_t)a * M + b] + Kbar[(size_t)b * M + a];
+  // Bbar (M x N), Fbar (N), Gs = Gbar + Gbar^T (N x N)
+  vector<real> Bb((size_t)M * N, 0.0), Fb(N, 0.0), Gs((size_t)N * N, 0.0), XK((size_t)M * N, 0.0), Xl(N, 0.0);
+  for (int a = 0; a < M; a++)
+    for (int b = 0; b < M; b++) {
+      const real k = Ks[(size_t)a * M + b];
+      if (k == 0.0) continue;
+      for (int i = 0; i < N; i++) XK[(size_t)a * N + i] += k * X[(size_t)b * N + i];  // rows of Ks X^T
+    }
+  for (int m = 0; m < M; m++)
+    for (int i = 0; i < N; i++) Xl[i] += X[(size_t)m * N + i] * lbar[m];
+  for (int m = 0; m < M; m++)
+    for (int i = 0; i < N; i++) Bb[(size_t)m * N + i] = XK[(size_t)m * N + i] + lbar[m] * y[i];
+  for (int i = 0; i < N; i++) Fb[i] = Xl[i];
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) {
+      real v = 0.0;
+      for (int m = 0; m < M; m++) v += X[(size_t)m * N + i] * XK[(size_t)m * N + j];
+      Gs[(size_t)i * N + j] = -(v + Xl[i] * y[j] + y[i] * Xl[j]);
+    }
+  std::fill(cbar, cbar + (size_t)P.desc.n_slots * Ptot, 0.0);
+  real nrm0[3] = {0, 0, 0};
+  vector<real> tmp(N), rvv(M);
+  // Gram points: dJ/dslot = wm sum_r dL_r^T Gs L_r
+  {
+    int nT = 0;
+    vector<int> row0(P.nIPterms + 1, 0);
+    for (int t = 0; t < P.nIPterms; t++) { row0[t] = nT; nT += P.ip_ncomp[t]; }
+    vector<real> Lq((size_t)nT * N), Y((size_t)nT * N);
+    for (int q = 0; q < QG; q++) {
+      Geo g;
+      geometry(P, nodes, &P.rG.pts[q * d], g);
+      const real wm = P.rG.wts[q] * g.det;
+      std::fill(Lq.begin(), Lq.end(), 0.0);
+      for (auto& e : P.ip) {
+        const VarLayout& TL = P.tv[e.test_var];
+        test_op_values(P, P.test_tab[e.test_var][0], q, e.test_op, g, nrm0, tmp.data());
+        real cf = e.coef * slotval(coeff, Ptot, e.slot, q);
+        for (int i = 0; i < TL.ndofs; i++) Lq[(size_t)(row0[e.term] + e.comp) * N + TL.offset + i] += cf * tmp[i];
+      }
+      for (int r = 0; r < nT; r++)
+        for (int i = 0; i < N; i++) {
+          real v = 0.0;
+          for (int j = 0; j < N; j++) v += Gs[(size_t)i * N + j] * Lq[(size_t)r * N + j];
+          Y[(size_t)r * N + i] = v;
+        }
+      for (auto& e : P.ip) {
+        if (e.slot < 0) continue;
+        const VarLayout& TL = P.tv[e.test_var];
+        test_op_values(P, P.test_tab[e.test_var][0], q, e.test_op, g, nrm0, tmp.data());
+        real v = 0.0;
+        for (int i = 0; i < TL.ndofs; i++) v += tmp[i] * Y[(size_t)(row0[e.term] + e.comp) * N + TL.offset + i];
+        cbar[(size_t)e.slot * Ptot + q] += wm * e.coef * v;
+      }
+    }
+  }
+  // B and F volume points
+  for (int q = 0; q < QB; q++) {
+    Geo g;
+    geometry(P, nodes, &P.rB.pts[q * d], g);
+    const real wm = P.rB.wts[q] * g.det;
+    const int p = QG + q;
+    for (auto& t : P.bf) {
+      if (t.boundary || t.slot < 0) continue;
+      const VarLayout& TL = P.tv[t.test_var];
+      const VarLayout& RL = P.rv[t.trial_var];
+      test_op_values(P, P.test_tab[t.test_var][1], q, t.test_op, g, nrm0, tmp.data());
+      field_values(RL, P.field_tab[t.trial_var][1], q, t.trial_op, rvv.data());
+      real v = 0.0;
+      for (int m = 0; m < RL.ndofs; m++) {
+        if (rvv[m] == 0.0) continue;
+        real w = 0.0;
+        for (int i = 0; i < TL.ndofs; i++) w += Bb[(size_t)(RL.offset + m) * N + TL.offset + i] * tmp[i];
+        v += rvv[m] * w;
+      }
+      cbar[(size_t)t.slot * Ptot + p] += wm * t.coef * v;
+    }
+    for (auto& r : P.rhs) {
+      if (r.slot < 0) continue;
+      const VarLayout& TL = P.tv[r.test_var];
+      test_op_values(P, P.test_tab[r.test_var][1], q, r.test_op, g, nrm0, tmp.data());
+      real v = 0.0;
+      for (int i = 0; i < TL.ndofs; i++) v += Fb[TL.offset + i] * tmp[i];
+      cbar[(size_t)r.slot * Ptot + p] += wm * r.coef * v;
+    }
+  }
+  // B side points
+  for (int sd = 0; sd < P.topo.nsides; sd++)
+    for (int q = 0; q < QS; q++) {
+      Geo g;
+      geometry(P, nodes, &P.side_pts[sd][q * d], g);
+      real meas, nrm[3];
+      side_geometry(P, g, sd, q, meas, nrm);
+      const real wm = P.rS.wts[q] * meas;
+      const int p = QG + QB + sd * QS + q;
+      for (auto& t : P.bf) {
+        if (!t.boundary || t.slot < 0) continue;
+        const VarLayout& TL = P.tv[t.test_var];
+        const VarLayout& RL = P.rv[t.trial_var];
+        test_op_values(P, P.test_tab[t.test_var][2 + sd], q, t.test_op, g, nrm, tmp.data());
+        real cf = wm * t.coef;
+        if (t.normal_comp >= 0) cf *= nrm[t.normal_comp];
+        int m0, mcount;
+        if (RL.kind == DPG_VAR_FIELD) {
+          field_values(RL, P.field_tab[t.trial_var][2 + sd], q, t.trial_op, rvv.data());
+          m0 = RL.offset; mcount = RL.ndofs;
+        } else {
+          const RefTab& TT = P.trace_tab[t.trial_var];
+          for (int m = 0; m < RL.per_side; m++) rvv[m] = TT.val[(size_t)q * TT.card + m];
+          if (RL.kind == DPG_VAR_FLUX) cf *= (real)parity[sd];
+          m0 = RL.offset + sd * RL.per_side; mcount = RL.per_side;
+        }
+        real v = 0.0;
+        for (int m = 0; m < mcount; m++) {
+          if (rvv[m] == 0.0) continue;
+          real w = 0.0;
+          for (int i = 0; i < TL.ndofs; i++) w += Bb[(size_t)(m0 + m) * N + TL.offset + i] * tmp[i];
+          v += rvv[m] * w;
+        }
+        cbar[(size_t)t.slot * Ptot + p] += cf * v;
+      }
+    }
+}
+
 // ----------------------------------------------------------------------------
 // Dense kernels, LAPACK semantics (column-major views)
 // ----------------------------------------------------------------------------
@@ -1435,6 +1610,132 @@ int orc_cell_operators(void* pp, const double* nodes, const int8_t* parity, cons
   narrow(L_, L); narrow(wm_, wm); narrow(U_, U); narrow(V_, V); narrow(fw_, fw); narrow(FV_, FV);
   for (size_t i = 0; i < rt.size(); i++) rterm[i] = rt[i];
   return 0;
+}
+
+// Hand gradient of J = sum_c <Kbar_c, K_c> + <lbar_c, l_c> with respect to the
+// coefficient slots: coeff_bar (C, n_slots, n_points_total).  Kbar (C, M, M), lbar (C, M).
+int orc_adjoint(void* pp, int C, const double* nodes, const int8_t* parity, const double* coeff, const double* Kbar,
+                const double* lbar, double* coeff_bar, int nthreads) {
+  Plan* p = (Plan*)pp;
+  const int M = p->M, nv = p->topo.nv, d = p->d, ns = p->topo.nsides;
+  dpg_plan_info pi;
+  orc_plan_query(pp, &pi);
+  const size_t cstride = (size_t)p->desc.n_slots * pi.n_points_total;
+  auto work = [&](int c0, int c1) {
+    for (int c = c0; c < c1; c++) {
+      vector<real> xn = widen(nodes + (size_t)c * nv * d, (size_t)nv * d);
+      vector<real> xc = coeff ? widen(coeff + c * cstride, cstride) : vector<real>();
+      vector<real> kb = widen(Kbar + (size_t)c * M * M, (size_t)M * M), lb = widen(lbar + (size_t)c * M, M);
+      vector<real> cb(cstride);
+      adjoint_cell(*p, xn.data(), parity + (size_t)c * ns, coeff ? xc.data() : nullptr, kb.data(), lb.data(), cb.data());
+      narrow(cb, coeff_bar + c * cstride);
+    }
+  };
+  if (nthreads <= 1 || C < 2) {
+    work(0, C);
+  } else {
+    std::vector<std::thread> th;
+    int per = (C + nthreads - 1) / nthreads;
+    for (int t = 0; t < nthreads; t++) {
+      int c0 = t * per, c1 = std::min(C, c0 + per);
+      if (c0 >= c1) break;
+      th.emplace_back(work, c0, c1);
+    }
+    for (auto& x : th) x.join();
+  }
+  return 0;
+}
+
+// J = sum_c <Kbar_c, K_c> + <lbar_c, l_c> computed in `real` and returned as the
+// unevaluated sum out[0] + out[1] of two doubles (out[0] = J rounded, out[1] = the
+// rest), so that differences of nearby losses keep the build's precision.
+int orc_loss(void* pp, int C, const double* nodes, const int8_t* parity, const double* coeff, const double* Kbar,
+             const double* lbar, double* out, int nthreads) {
+  Plan* p = (Plan*)pp;
+  const int N = p->N, M = p->M, nv = p->topo.nv, d = p->d, ns = p->topo.nsides;
+  dpg_plan_info pi;
+  orc_plan_query(pp, &pi);
+  const size_t cstride = (size_t)p->desc.n_slots * pi.n_points_total;
+  vector<real> part(std::max(1, nthreads), 0.0);
+  auto work = [&](int t, int c0, int c1) {
+    CellOut o;
+    vector<real> Kc((size_t)M * M), lc(M);
+    real acc = 0.0;
+    for (int c = c0; c < c1; c++) {
+      vector<real> xn = widen(nodes + (size_t)c * nv * d, (size_t)nv * d);
+      vector<real> xc = coeff ? widen(coeff + c * cstride, cstride) : vector<real>();
+      assemble_cell(*p, xn.data(), parity + (size_t)c * ns, coeff ? xc.data() : nullptr, o);
+      factored_cholesky_solve(N, M, o.G.data(), o.B.data(), o.F.data(), Kc.data(), lc.data());
+      for (size_t k = 0; k < (size_t)M * M; k++) acc += (real)Kbar[(size_t)c * M * M + k] * Kc[k];
+      for (int k = 0; k < M; k++) acc += (real)lbar[(size_t)c * M + k] * lc[k];
+    }
+    part[t] = acc;
+  };
+  if (nthreads <= 1 || C < 2) {
+    work(0, 0, C);
+  } else {
+    std::vector<std::thread> th;
+    int per = (C + nthreads - 1) / nthreads;
+    for (int t = 0; t < nthreads; t++) {
+      int c0 = t * per, c1 = std::min(C, c0 + per);
+      if (c0 >= c1) break;
+      th.emplace_back(work, t, c0, c1);
+    }
+    for (auto& x : th) x.join();
+  }
+  real tot = 0.0;
+  for (auto v : part) tot += v;
+  out[0] = (double)tot;
+  out[1] = (double)(tot - (real)out[0]);
+  return 0;
+}
+
+// Central difference (J(coeff + h dir) - J(coeff - h dir)) / (2 h) of
+// J = sum_c <Kbar_c, K_c> + <lbar_c, l_c>, computed entirely in `real` (the perturbed
+// coefficients, both assemblies and the difference), so that in the __float128 build the
+// result carries the difference's truncation error only.
+double orc_fd_directional(void* pp, int C, const double* nodes, const int8_t* parity, const double* coeff,
+                          const double* dir, double h, const double* Kbar, const double* lbar, int nthreads) {
+  Plan* p = (Plan*)pp;
+  const int N = p->N, M = p->M, nv = p->topo.nv, d = p->d, ns = p->topo.nsides;
+  dpg_plan_info pi;
+  orc_plan_query(pp, &pi);
+  const size_t cstride = (size_t)p->desc.n_slots * pi.n_points_total;
+  vector<real> part(std::max(1, nthreads), 0.0);
+  auto work = [&](int t, int c0, int c1) {
+    CellOut o;
+    vector<real> Kc((size_t)M * M), lc(M);
+    real acc = 0.0;
+    for (int c = c0; c < c1; c++) {
+      vector<real> xn = widen(nodes + (size_t)c * nv * d, (size_t)nv * d);
+      for (int sg = -1; sg <= 1; sg += 2) {
+        vector<real> xc(cstride);
+        for (size_t k = 0; k < cstride; k++) xc[k] = (real)coeff[c * cstride + k] + sg * (real)h * (real)dir[c * cstride + k];
+        assemble_cell(*p, xn.data(), parity + (size_t)c * ns, xc.data(), o);
+        factored_cholesky_solve(N, M, o.G.data(), o.B.data(), o.F.data(), Kc.data(), lc.data());
+        real J = 0.0;
+        for (size_t k = 0; k < (size_t)M * M; k++) J += (real)Kbar[(size_t)c * M * M + k] * Kc[k];
+        for (int k = 0; k < M; k++) J += (real)lbar[(size_t)c * M + k] * lc[k];
+        acc += sg * J;
+      }
+    }
+    part[t] = acc;
+  };
+  if (nthreads <= 1 || C < 2) {
+    work(0, 0, C);
+  } else {
+    std::vector<std::thread> th;
+    int per = (C + nthreads - 1) / nthreads;
+    for (int t = 0; t < nthreads; t++) {
+      int c0 = t * per, c1 = std::min(C, c0 + per);
+      if (c0 >= c1) break;
+      th.emplace_back(work, t, c0, c1);
+    }
+    for (auto& x : th) x.join();
+  }
+  real tot = 0.0;
+  for (auto v : part) tot += v;
+  return (double)(tot / (2 * (real)h));
 }
 
 // Single-cell factored Cholesky (inputs copied): G row-major NxN, B (M,N), F (N).

@@ -45,6 +45,10 @@ def lib(xp=False):
         L.orc_tri_cubature.argtypes = [ct.c_int, ct.c_void_p, ct.c_void_p]
         L.orc_tri_nodes.argtypes = [ct.c_int, ct.c_void_p]
         L.orc_cell_operators.argtypes = [ct.c_void_p] * 12
+        L.orc_adjoint.argtypes = [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 6 + [ct.c_int]
+        L.orc_fd_directional.argtypes = [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 4 + [ct.c_double] + [ct.c_void_p] * 2 + [ct.c_int]
+        L.orc_fd_directional.restype = ct.c_double
+        L.orc_loss.argtypes = [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 6 + [ct.c_int]
         L.orc_last_error.restype = ct.c_char_p
         assert L.orc_precision() == (1 if xp else 0)
         _LIBS[xp] = L
@@ -100,6 +104,33 @@ class OraclePlan:
                            _p(out.get("F")), _p(out["K"]), _p(out["l"]), _p(out["S"]), _p(out["s"]),
                            _p(out["info"]), nthreads)
         return out
+
+    def adjoint(self, nodes, parity, coeff, Kbar, lbar, nthreads=1):
+        """Hand gradient of J = sum_c <Kbar_c, K_c> + <lbar_c, l_c> with respect to the
+        coefficient slots, (C, n_slots, n_points_total)."""
+        C = nodes.shape[0]
+        cbar = np.zeros((C, self.info["n_slots"], self.info["n_points_total"]))
+        arr = lambda a, t=np.float64: np.ascontiguousarray(a, dtype=t)  # noqa: E731
+        self.L.orc_adjoint(self.h, C, _p(arr(nodes)), _p(arr(parity, np.int8)), _p(arr(coeff)), _p(arr(Kbar)),
+                           _p(arr(lbar)), _p(cbar), nthreads)
+        return cbar
+
+    def loss(self, nodes, parity, coeff, Kbar, lbar, nthreads=1):
+        """J = sum_c <Kbar_c, K_c> + <lbar_c, l_c> as an unevaluated pair of doubles (hi, lo)."""
+        arr = lambda a, t=np.float64: np.ascontiguousarray(a, dtype=t)  # noqa: E731
+        out = np.zeros(2)
+        self.L.orc_loss(self.h, nodes.shape[0], _p(arr(nodes)), _p(arr(parity, np.int8)), _p(arr(coeff)),
+                        _p(arr(Kbar)), _p(arr(lbar)), _p(out), nthreads)
+        return float(out[0]), float(out[1])
+
+    def fd_directional(self, nodes, parity, coeff, direction, h, Kbar, lbar, nthreads=1):
+        """Central difference of J = sum_c <Kbar_c, K_c> + <lbar_c, l_c> along `direction`
+        (same shape as coeff) with step h, all in the build's arithmetic (xp=True: the
+        perturbed coefficients and the difference in __float128)."""
+        arr = lambda a, t=np.float64: np.ascontiguousarray(a, dtype=t)  # noqa: E731
+        return float(self.L.orc_fd_directional(self.h, nodes.shape[0], _p(arr(nodes)), _p(arr(parity, np.int8)),
+                                               _p(arr(coeff)), _p(arr(direction)), float(h), _p(arr(Kbar)),
+                                               _p(arr(lbar)), nthreads))
 
     def operators(self, nodes, parity, coeff=None):
         """Quadrature operator rows of ONE cell (nodes (nv, d), parity (ns,), coeff

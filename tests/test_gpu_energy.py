@@ -10,7 +10,7 @@ import pytest
 torch = pytest.importorskip("torch")
 
 from camellia2_b200 import lib as dlib  # noqa: E402
-from tests.helpers import cdr2d, coeffs_for, poisson2d, poisson3d  # noqa: E402
+from tests.helpers import cdr2d, coeffs_for, poisson2d, poisson3d, stokes2d  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -54,3 +54,27 @@ def test_energy_error_of_exact_solution_vanishes(oracle_mod):
     e_rand, _ = plan.energy_error(_dev(nodes), _dev(par), _dev(co), _dev(xr))
     torch.cuda.synchronize()
     assert float(e.max()) < 1e-10 * float(e_rand.min())
+
+
+@pytest.mark.parametrize("make", [lambda: poisson2d(2, 2, 2, 2, 0.1), lambda: stokes2d(3, 2, 2, 1, 0.1)],
+                         ids=["single_cta", "large_bucket"])
+def test_energy_error_is_nan_where_the_factorisation_fails(make):
+    """Cells mirrored in x have det J < 0, so their Gram matrix is negative definite and its
+    factorisation fails (info != 0): the energy error there is NaN, the other cells' are
+    unchanged."""
+    form, bucket, nodes, par = make()
+    plan = dlib.Plan(bucket)
+    C, M = nodes.shape[0], plan.info["M"]
+    co = coeffs_for(bucket, plan.info, C)
+    x = np.random.default_rng(4).normal(size=(C, M))
+    bad = nodes.copy()
+    bad[1, :, 0] = -bad[1, :, 0]  # cell 1 mirrored: negative Jacobian determinant
+    dco = None if co is None else _dev(co)
+    e0, info0 = plan.energy_error(_dev(nodes), _dev(par), dco, _dev(x))
+    e1, info1 = plan.energy_error(_dev(bad), _dev(par), dco, _dev(x))
+    torch.cuda.synchronize()
+    e0, e1, info0, info1 = (t.cpu().numpy() for t in (e0, e1, info0, info1))
+    assert (info0 == 0).all() and np.isfinite(e0).all()
+    assert info1[1] != 0 and np.isnan(e1[1])
+    keep = np.arange(C) != 1
+    assert (info1[keep] == 0).all() and np.array_equal(e1[keep], e0[keep])

@@ -158,3 +158,14 @@ def test_invalid_descriptor_is_rejected():
     with pytest.raises(dlib.DpgError) as e:
         dlib.Plan(h)
     assert e.value.code == abi.DPG_ERR_INVALID_ARGUMENT
+
+
+def test_mixed_precision_is_refused():
+    """No mixed-precision form is built: a plan asking for one is refused with
+    DPG_ERR_UNSUPPORTED instead of silently running the FP64 form."""
+    from camellia2_b200 import formulation as fm
+    bucket = fm.PoissonFormulation(3).bucket(abi.TOPO_HEX, 2, 1, precision=abi.PREC_MIXED)
+    with pytest.raises(dlib.DpgError) as e:
+        dlib.Plan(bucket)
+    assert e.value.code == abi.DPG_ERR_UNSUPPORTED
+    assert "DPG_PREC_MIXED" in str(e.value)
