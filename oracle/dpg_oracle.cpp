@@ -1490,6 +1490,201 @@ int condense(int M, const int* is_field, const real* K, const real* l, real* S, 
   return err ? -err : 0;
 }
 
+#ifndef ORC_QUAD
+// ----------------------------------------------------------------------------
+// Fast mode: the CPU baseline.  The same algorithm with Camellia's cost structure:
+// every quadrature contraction is one DGEMM per block, as Intrepid's
+// FunctionSpaceTools::integrate(COMP_BLAS) does per (trial var, test var) pair
+// (LinearTerm.cpp:574-576) -- G per graph-norm term and var pair, B per bilinear term
+// (and side), F by DGEMV -- then DPOTRF, DTRSM, DSYRK and DGEMV as in
+// BF.cpp:944-1016.  The BLAS/LAPACK routines are the caller's (the tests and the bench
+// hand over scipy's OpenBLAS through scipy.linalg.cython_blas / cython_lapack, one
+// thread per call).
+// ----------------------------------------------------------------------------
+typedef void (*DgemmFn)(const char*, const char*, const int*, const int*, const int*, const double*, const double*,
+                        const int*, const double*, const int*, const double*, double*, const int*);
+typedef void (*DgemvFn)(const char*, const int*, const int*, const double*, const double*, const int*, const double*,
+                        const int*, const double*, double*, const int*);
+typedef void (*DsyrkFn)(const char*, const char*, const int*, const int*, const double*, const double*, const int*,
+                        const double*, double*, const int*);
+typedef void (*DtrsmFn)(const char*, const char*, const char*, const char*, const int*, const int*, const double*,
+                        const double*, const int*, double*, const int*);
+typedef void (*DpotrfFn)(const char*, const int*, double*, const int*, int*);
+struct BlasFns {
+  DgemmFn dgemm = nullptr;
+  DgemvFn dgemv = nullptr;
+  DsyrkFn dsyrk = nullptr;
+  DtrsmFn dtrsm = nullptr;
+  DpotrfFn dpotrf = nullptr;
+};
+static BlasFns g_blas;
+
+// One cell: K (M x M row-major), l (M), S, s (nullable), returns INFO.
+static int assemble_cell_blas(const Plan& P, const double* nodes, const int8_t* parity, const double* coeff,
+                              double* K, double* l, double* S, double* s) {
+  const BlasFns& b = g_blas;
+  const int N = P.N, M = P.M, d = P.d;
+  const int QG = P.rG.npts(), QB = P.rB.npts(), QS = P.rS.npts(), ns = P.topo.nsides;
+  const int Ptot = QG + QB + ns * QS;
+  const double one = 1.0, zero = 0.0;
+  const int ione = 1;
+  double nrm0[3] = {0, 0, 0};
+  vector<double> G((size_t)N * N, 0.0), B((size_t)M * N, 0.0), F(N, 0.0), tmp(N), rvv(M);
+  // geometry at the Gram points
+  vector<Geo> gG(QG);
+  vector<double> wG(QG);
+  for (int q = 0; q < QG; q++) {
+    geometry(P, nodes, &P.rG.pts[q * d], gG[q]);
+    wG[q] = P.rG.wts[q] * gG[q].det;
+  }
+  // G: per term, values of each of its vars over (point, component), k fastest
+  for (int t = 0; t < P.nIPterms; t++) {
+    const int nc = P.ip_ncomp[t], Kt = QG * nc;
+    vector<int> vars;
+    for (auto& e : P.ip)
+      if (e.term == t && std::find(vars.begin(), vars.end(), e.test_var) == vars.end()) vars.push_back(e.test_var);
+    std::sort(vars.begin(), vars.end());
+    vector<vector<double>> val(vars.size()), wval(vars.size());
+    for (size_t a = 0; a < vars.size(); a++) {
+      const VarLayout& TL = P.tv[vars[a]];
+      val[a].assign((size_t)TL.ndofs * Kt, 0.0);
+      for (auto& e : P.ip) {
+        if (e.term != t || e.test_var != vars[a]) continue;
+        for (int q = 0; q < QG; q++) {
+          test_op_values(P, P.test_tab[e.test_var][0], q, e.test_op, gG[q], nrm0, tmp.data());
+          const double cf = e.coef * slotval(coeff, Ptot, e.slot, q);
+          for (int i = 0; i < TL.ndofs; i++) val[a][(size_t)i * Kt + q * nc + e.comp] += cf * tmp[i];
+        }
+      }
+      wval[a] = val[a];
+      for (int i = 0; i < TL.ndofs; i++)
+        for (int q = 0; q < QG; q++)
+          for (int c = 0; c < nc; c++) wval[a][(size_t)i * Kt + q * nc + c] *= wG[q];
+    }
+    vector<double> mini;
+    for (size_t a = 0; a < vars.size(); a++)
+      for (size_t c2 = 0; c2 < vars.size(); c2++) {
+        const VarLayout& U = P.tv[vars[a]];
+        const VarLayout& V = P.tv[vars[c2]];
+        const int nu = U.ndofs, nv = V.ndofs;
+        mini.assign((size_t)nu * nv, 0.0);
+        b.dgemm("T", "N", &nu, &nv, &Kt, &one, wval[a].data(), &Kt, val[c2].data(), &Kt, &zero, mini.data(), &nu);
+        for (int j = 0; j < nv; j++)
+          for (int i = 0; i < nu; i++) G[(size_t)(U.offset + i) * N + V.offset + j] += mini[(size_t)j * nu + i];
+      }
+  }
+  // B and F: volume terms, one DGEMM per term over the B points
+  {
+    vector<Geo> gB(QB);
+    vector<double> wB(QB);
+    for (int q = 0; q < QB; q++) {
+      geometry(P, nodes, &P.rB.pts[q * d], gB[q]);
+      wB[q] = P.rB.wts[q] * gB[q].det;
+    }
+    for (auto& t : P.bf) {
+      if (t.boundary) continue;
+      const VarLayout& TL = P.tv[t.test_var];
+      const VarLayout& RL = P.rv[t.trial_var];
+      const int mu = RL.ndofs, nv = TL.ndofs;
+      vector<double> Uw((size_t)mu * QB), Vt((size_t)nv * QB), blk((size_t)mu * nv);
+      for (int q = 0; q < QB; q++) {
+        test_op_values(P, P.test_tab[t.test_var][1], q, t.test_op, gB[q], nrm0, tmp.data());
+        field_values(RL, P.field_tab[t.trial_var][1], q, t.trial_op, rvv.data());
+        const double cf = wB[q] * t.coef * slotval(coeff, Ptot, t.slot, QG + q);
+        for (int m = 0; m < mu; m++) Uw[(size_t)m * QB + q] = cf * rvv[m];
+        for (int i = 0; i < nv; i++) Vt[(size_t)i * QB + q] = tmp[i];
+      }
+      b.dgemm("T", "N", &mu, &nv, &QB, &one, Uw.data(), &QB, Vt.data(), &QB, &zero, blk.data(), &mu);
+      for (int i = 0; i < nv; i++)
+        for (int m = 0; m < mu; m++) B[(size_t)(RL.offset + m) * N + TL.offset + i] += blk[(size_t)i * mu + m];
+    }
+    for (auto& r : P.rhs) {
+      const VarLayout& TL = P.tv[r.test_var];
+      const int nv = TL.ndofs;
+      vector<double> Vt((size_t)QB * nv), fw(QB), out(nv);
+      for (int q = 0; q < QB; q++) {
+        test_op_values(P, P.test_tab[r.test_var][1], q, r.test_op, gB[q], nrm0, tmp.data());
+        fw[q] = wB[q] * r.coef * slotval(coeff, Ptot, r.slot, QG + q);
+        for (int i = 0; i < nv; i++) Vt[(size_t)i * QB + q] = tmp[i];
+      }
+      b.dgemv("T", &QB, &nv, &one, Vt.data(), &QB, fw.data(), &ione, &zero, out.data(), &ione);
+      for (int i = 0; i < nv; i++) F[TL.offset + i] += out[i];
+    }
+  }
+  // B: side terms, one DGEMM per (term, side) over the side points
+  for (int sd = 0; sd < ns; sd++) {
+    vector<Geo> gS(QS);
+    vector<double> wS(QS), nS((size_t)QS * 3);
+    for (int q = 0; q < QS; q++) {
+      geometry(P, nodes, &P.side_pts[sd][q * d], gS[q]);
+      double meas;
+      side_geometry(P, gS[q], sd, q, meas, &nS[(size_t)q * 3]);
+      wS[q] = P.rS.wts[q] * meas;
+    }
+    for (auto& t : P.bf) {
+      if (!t.boundary) continue;
+      const VarLayout& TL = P.tv[t.test_var];
+      const VarLayout& RL = P.rv[t.trial_var];
+      const bool field = RL.kind == DPG_VAR_FIELD;
+      const int mu = field ? RL.ndofs : RL.per_side, m0 = field ? RL.offset : RL.offset + sd * RL.per_side;
+      const int nv = TL.ndofs;
+      vector<double> Uw((size_t)mu * QS), Vt((size_t)nv * QS), blk((size_t)mu * nv);
+      for (int q = 0; q < QS; q++) {
+        test_op_values(P, P.test_tab[t.test_var][2 + sd], q, t.test_op, gS[q], &nS[(size_t)q * 3], tmp.data());
+        double cf = wS[q] * t.coef * slotval(coeff, Ptot, t.slot, QG + QB + sd * QS + q);
+        if (t.normal_comp >= 0) cf *= nS[(size_t)q * 3 + t.normal_comp];
+        if (field) {
+          field_values(RL, P.field_tab[t.trial_var][2 + sd], q, t.trial_op, rvv.data());
+        } else {
+          const RefTab& TT = P.trace_tab[t.trial_var];
+          for (int m = 0; m < mu; m++) rvv[m] = TT.val[(size_t)q * TT.card + m];
+          if (RL.kind == DPG_VAR_FLUX) cf *= (double)parity[sd];
+        }
+        for (int m = 0; m < mu; m++) Uw[(size_t)m * QS + q] = cf * rvv[m];
+        for (int i = 0; i < nv; i++) Vt[(size_t)i * QS + q] = tmp[i];
+      }
+      b.dgemm("T", "N", &mu, &nv, &QS, &one, Uw.data(), &QS, Vt.data(), &QS, &zero, blk.data(), &mu);
+      for (int i = 0; i < nv; i++)
+        for (int m = 0; m < mu; m++) B[(size_t)(m0 + m) * N + TL.offset + i] += blk[(size_t)i * mu + m];
+    }
+  }
+  // factored Cholesky solve (BF.cpp:944-1016); G row-major = column-major transpose, symmetric
+  vector<double> sc(N);
+  for (int i = 0; i < N; i++) {
+    const double gii = G[(size_t)i * N + i];
+    if (!(gii > 0.0)) return i + 1;
+    sc[i] = 1.0 / std::sqrt(gii);
+  }
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < N; j++) G[(size_t)i * N + j] *= sc[i] * sc[j];
+  int info = 0;
+  b.dpotrf("U", &N, G.data(), &N, &info);  // row-major lower = column-major upper
+  if (info != 0) return info;
+  // L (column-major lower) = transpose of the row-major upper factor: unscale L(i,j) /= s_i
+  vector<double> L((size_t)N * N, 0.0);
+  for (int j = 0; j < N; j++)
+    for (int i = j; i < N; i++) L[(size_t)j * N + i] = G[(size_t)i * N + j] / sc[i];
+  b.dtrsm("L", "L", "N", "N", &N, &M, &one, L.data(), &N, B.data(), &N);  // W = L^-1 B^T (N x M, ld N)
+  vector<double> Kc((size_t)M * M, 0.0);
+  b.dsyrk("L", "T", &M, &N, &one, B.data(), &N, &zero, Kc.data(), &M);   // K = W^T W (lower, column-major)
+  for (int j = 0; j < M; j++)
+    for (int i = j; i < M; i++) {
+      K[(size_t)i * M + j] = Kc[(size_t)j * M + i];
+      K[(size_t)j * M + i] = Kc[(size_t)j * M + i];
+    }
+  b.dtrsm("L", "L", "N", "N", &N, &ione, &one, L.data(), &N, F.data(), &N);  // y = L^-1 F
+  b.dgemv("T", &N, &M, &one, B.data(), &N, F.data(), &ione, &zero, l, &ione);  // l = W^T y
+  if (S || s) {
+    vector<double> S_((size_t)P.nt * P.nt), s_(P.nt);
+    int r = condense(M, P.is_field.data(), K, l, S_.data(), s_.data());
+    if (S) std::copy(S_.begin(), S_.end(), S);
+    if (s) std::copy(s_.begin(), s_.end(), s);
+    if (r != 0) return r;
+  }
+  return 0;
+}
+#endif  // ORC_QUAD
+
 }  // namespace ORC_NS
 
 // ----------------------------------------------------------------------------
@@ -1737,6 +1932,56 @@ double orc_fd_directional(void* pp, int C, const double* nodes, const int8_t* pa
   for (auto v : part) tot += v;
   return (double)(tot / (2 * (real)h));
 }
+
+#ifndef ORC_QUAD
+// BLAS/LAPACK entry points for the fast mode (Fortran LP64 interface; any NULL
+// disables it).  Returns 0 when the fast mode is available.
+int orc_set_blas(void* dgemm, void* dgemv, void* dsyrk, void* dtrsm, void* dpotrf) {
+  g_blas.dgemm = (DgemmFn)dgemm;
+  g_blas.dgemv = (DgemvFn)dgemv;
+  g_blas.dsyrk = (DsyrkFn)dsyrk;
+  g_blas.dtrsm = (DtrsmFn)dtrsm;
+  g_blas.dpotrf = (DpotrfFn)dpotrf;
+  return (dgemm && dgemv && dsyrk && dtrsm && dpotrf) ? 0 : 1;
+}
+
+// Fast mode (the CPU baseline): K, l, S, s, info of C cells on nthreads threads.
+int orc_assemble_blas(void* pp, int C, const double* nodes, const int8_t* parity, const double* coeff, double* K,
+                      double* l, double* S, double* s, int32_t* info, int nthreads) {
+  if (!g_blas.dgemm || !g_blas.dgemv || !g_blas.dsyrk || !g_blas.dtrsm || !g_blas.dpotrf) {
+    g_err = "orc_assemble_blas: BLAS entry points not set (orc_set_blas)";
+    return 1;
+  }
+  Plan* p = (Plan*)pp;
+  const int M = p->M, nt = p->nt, nv = p->topo.nv, d = p->d, ns = p->topo.nsides;
+  dpg_plan_info pi;
+  orc_plan_query(pp, &pi);
+  const size_t cstride = (size_t)p->desc.n_slots * pi.n_points_total;
+  auto work = [&](int c0, int c1) {
+    vector<double> Kc((size_t)M * M), lc(M);
+    for (int c = c0; c < c1; c++) {
+      int r = assemble_cell_blas(*p, nodes + (size_t)c * nv * d, parity + (size_t)c * ns,
+                                 coeff ? coeff + c * cstride : nullptr, K ? K + (size_t)c * M * M : Kc.data(),
+                                 l ? l + (size_t)c * M : lc.data(), S ? S + (size_t)c * nt * nt : nullptr,
+                                 s ? s + (size_t)c * nt : nullptr);
+      if (info) info[c] = r;
+    }
+  };
+  if (nthreads <= 1 || C < 2) {
+    work(0, C);
+  } else {
+    std::vector<std::thread> th;
+    int per = (C + nthreads - 1) / nthreads;
+    for (int t = 0; t < nthreads; t++) {
+      int c0 = t * per, c1 = std::min(C, c0 + per);
+      if (c0 >= c1) break;
+      th.emplace_back(work, c0, c1);
+    }
+    for (auto& x : th) x.join();
+  }
+  return 0;
+}
+#endif  // ORC_QUAD
 
 // Single-cell factored Cholesky (inputs copied): G row-major NxN, B (M,N), F (N).
 int orc_factored_cholesky_solve(int N, int M, const double* G, const double* B, const double* F, double* K,

@@ -49,6 +49,9 @@ def lib(xp=False):
         L.orc_fd_directional.argtypes = [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 4 + [ct.c_double] + [ct.c_void_p] * 2 + [ct.c_int]
         L.orc_fd_directional.restype = ct.c_double
         L.orc_loss.argtypes = [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 6 + [ct.c_int]
+        if not xp:
+            L.orc_set_blas.argtypes = [ct.c_void_p] * 5
+            L.orc_assemble_blas.argtypes = [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 8 + [ct.c_int]
         L.orc_last_error.restype = ct.c_char_p
         assert L.orc_precision() == (1 if xp else 0)
         _LIBS[xp] = L
@@ -57,6 +60,32 @@ def lib(xp=False):
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+_BLAS_READY = False
+
+
+def enable_blas():
+    """Hand scipy's BLAS/LAPACK (scipy.linalg.cython_blas / cython_lapack: the OpenBLAS
+    scipy bundles, Fortran LP64 interface) to the FP64 oracle's fast mode."""
+    global _BLAS_READY
+    if _BLAS_READY:
+        return
+    import scipy.linalg.cython_blas as cb
+    import scipy.linalg.cython_lapack as cl
+    get_name = ct.pythonapi.PyCapsule_GetName
+    get_name.restype, get_name.argtypes = ct.c_char_p, [ct.py_object]
+    get_ptr = ct.pythonapi.PyCapsule_GetPointer
+    get_ptr.restype, get_ptr.argtypes = ct.c_void_p, [ct.py_object, ct.c_char_p]
+
+    def fn(mod, name):
+        cap = mod.__pyx_capi__[name]
+        return get_ptr(cap, get_name(cap))
+
+    ptrs = [fn(cb, "dgemm"), fn(cb, "dgemv"), fn(cb, "dsyrk"), fn(cb, "dtrsm"), fn(cl, "dpotrf")]
+    if lib().orc_set_blas(*[ct.c_void_p(x) for x in ptrs]) != 0:
+        raise RuntimeError("oracle fast mode: BLAS entry points missing")
+    _BLAS_READY = True
 
 
 class OraclePlan:
@@ -148,6 +177,27 @@ class OraclePlan:
                    U=np.zeros((nB, M)), V=np.zeros((nB, N)), fw=np.zeros(nF), FV=np.zeros((nF, N)))
         self.L.orc_cell_operators(self.h, _p(nodes), _p(parity), _p(cf), _p(dims),
                                   *(_p(out[k]) for k in ("L", "wm", "rterm", "U", "V", "fw", "FV")))
+        return out
+
+    def assemble_blas(self, nodes, parity, coeff=None, nthreads=1):
+        """Fast mode (the CPU baseline): the same outputs with every quadrature contraction a
+        DGEMM per block and the dense solve in LAPACK/BLAS, each call on one BLAS thread
+        (threads = cells in parallel)."""
+        from threadpoolctl import threadpool_limits
+        assert not self.xp
+        enable_blas()
+        i = self.info
+        C = nodes.shape[0]
+        M, t = i["M"], i["n_trace"]
+        arr = lambda a, ty=np.float64: np.ascontiguousarray(a, dtype=ty)  # noqa: E731
+        out = dict(K=np.zeros((C, M, M)), l=np.zeros((C, M)), S=np.zeros((C, t, t)), s=np.zeros((C, t)),
+                   info=np.zeros(C, dtype=np.int32))
+        with threadpool_limits(limits=1, user_api="blas"):
+            rc = self.L.orc_assemble_blas(self.h, C, _p(arr(nodes)), _p(arr(parity, np.int8)),
+                                          _p(None if coeff is None else arr(coeff)), _p(out["K"]), _p(out["l"]),
+                                          _p(out["S"]), _p(out["s"]), _p(out["info"]), nthreads)
+        if rc != 0:
+            raise RuntimeError(self.L.orc_last_error().decode())
         return out
 
     def parts(self, nodes, parity, coeff=None):
