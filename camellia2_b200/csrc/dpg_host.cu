@@ -1527,6 +1527,40 @@ const char* dpg_last_error_string(void) { return g_last_error.c_str(); }
 
 const char* dpg_version(void) { return "camellia2_b200 dpg 1 (sm_100a, FP64 DMMA)"; }
 
+int dpg_basis_tabulate(int topology, int space, int n, int npts, const double* pts, double* out) {
+  TopoData T;
+  if (!topo_data(topology, T)) return -fail(DPG_ERR_INVALID_ARGUMENT, "unknown topology");
+  if (npts < 0 || (npts > 0 && (!pts || !out))) return -fail(DPG_ERR_INVALID_ARGUMENT, "null argument");
+  const int dim = T.d;
+  int card;
+  if (space == DPG_SPACE_HGRAD) {
+    if (n < 0) return -fail(DPG_ERR_INVALID_ARGUMENT, "HGRAD order must be >= 0");
+    card = card_hgrad_t(topology, dim, n);
+  } else if (space == DPG_SPACE_HDIV) {
+    if (n < 1) return -fail(DPG_ERR_INVALID_ARGUMENT, "HDIV order must be >= 1");
+    card = card_hdiv_t(topology, dim, n);
+  } else {
+    return -fail(DPG_ERR_INVALID_ARGUMENT, "space must be HGRAD or HDIV");
+  }
+  std::vector<double> buf((size_t)card * (dim + 1));
+  for (int q = 0; q < npts; q++) {
+    if (space == DPG_SPACE_HGRAD) tab_hgrad_t(topology, dim, n, pts + (size_t)q * dim, buf.data());
+    else tab_hdiv_t(topology, dim, n, pts + (size_t)q * dim, buf.data());
+    std::copy(buf.begin(), buf.end(), out + (size_t)q * card * (dim + 1));
+  }
+  return card;
+}
+
+int dpg_cubature(int topology, int degree, double* pts, double* wts) {
+  TopoData T;
+  if (!topo_data(topology, T)) return -fail(DPG_ERR_INVALID_ARGUMENT, "unknown topology");
+  if (degree < 0) return -fail(DPG_ERR_INVALID_ARGUMENT, "degree must be >= 0");
+  const Rule r = topology == DPG_TOPO_TRI ? tri_rule(degree) : tensor_rule(T.d, degree);
+  if (pts) std::copy(r.x.begin(), r.x.end(), pts);
+  if (wts) std::copy(r.w.begin(), r.w.end(), wts);
+  return r.n;
+}
+
 int dpg_plan_create(const dpg_bucket_desc* desc, dpg_plan** out) {
   if (!desc || !out) return fail(DPG_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;

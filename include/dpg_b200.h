@@ -394,6 +394,23 @@ int dpg_assemble_noalloc(dpg_plan* plan, int C, const double* nodes, const int8_
                          const double* coeff, double* K, double* l, double* S, double* s,
                          int32_t* info, void* stream, int flags);
 
+/* The reference bases and cubature rules the plans are built from, for checking
+ * their conventions (host only; no GPU needed).  No counterpart in the reference as
+ * a C call: they tabulate what Camellia gets from Intrepid through BasisFactory
+ * (src/Basis/BasisFactory.cpp:122-420) and CubatureFactory
+ * (src/Basis/CubatureFactory.cpp:25-53).
+ * dpg_basis_tabulate: space DPG_SPACE_HGRAD (order n >= 0: Cn, nodal at the
+ * Gauss-Lobatto points of [-1,1]^d, x fastest; triangles: the warp & blend lattice
+ * on (0,0),(1,0),(0,1)) or DPG_SPACE_HDIV (order n >= 1: In, component-major; on
+ * triangles RT_n).  out holds, per point and dof, d + 1 doubles: HGRAD value and
+ * the d reference derivatives, HDIV the d value components and the divergence.
+ * Returns the cardinality, or -(DPG_ERR_*) on an invalid argument.
+ * dpg_cubature: the rule exact to `degree` (tensor Gauss on [-1,1]^d, collapsed
+ * Gauss on the triangle); pts (npts, d) and wts (npts) may be NULL; returns npts,
+ * or -(DPG_ERR_*) on an invalid argument. */
+int dpg_basis_tabulate(int topology, int space, int n, int npts, const double* pts, double* out);
+int dpg_cubature(int topology, int degree, double* pts, double* wts);
+
 /* Thread-local description of the last error. */
 const char* dpg_last_error_string(void);
 
