@@ -175,10 +175,11 @@ def other_configs(torch):
 def c3_forest(torch, timeit, dev, total=100_000):
     """The uneven-cell Stokes VGP workload: ~100k cells (70 % quads, 30 % triangles, p uniform
     on 1..6, Delta p = 2, refinement level geometric on 0..4, jittered), twelve (topology, p)
-    buckets in one CUDA graph: the single-CTA buckets in one persistent launch, the large ones
-    (quads p >= 3, triangles p >= 4) on the large-bucket kernel after it.  Each single-CTA
-    bucket's Gram staging chunk is picked by dpg_plan_autotune on its own cells first.
-    Per-bucket device times come from single-bucket launches."""
+    buckets in ONE persistent launch with a dynamic work queue (single-CTA and large buckets
+    alike, longest cells first), captured in a CUDA graph.  Tuned first: each bucket's shape by
+    dpg_plan_autotune on its own cells (Gram staging chunk for single-CTA buckets, formation
+    k-chunk for large ones), then the queue's claim size by dpg_multi_autotune.  Per-bucket
+    device times come from single-bucket launches."""
     from camellia2_b200 import formulation as fm, lib, mesh
     form = fm.StokesVGPFormulation(2)
     items, keys, per = [], [], {}
@@ -191,16 +192,20 @@ def c3_forest(torch, timeit, dev, total=100_000):
     for key, (pl, dn, dp, dc, out) in zip(keys, items):
         C = dn.shape[0]
         N, M = pl.info["N"], pl.info["M"]
-        chunk = pl.autotune(dn, dp, dc)  # per-bucket Gram staging chunk, timed on these cells
+        shape = pl.autotune(dn, dp, dc)  # per-bucket shape, timed on these cells
+        big = shape in (16, 32)  # formation k-chunk of a large-bucket plan (Gram chunks are 8 or 4)
         ms = timeit(lambda: pl.assemble(dn, dp, dc, out=out), reps=1)
         per[key] = {"cells": C, "N": N, "M": M, "ms": round(ms, 3), "cells_per_s": round(C / ms * 1e3),
-                    "kernel": "single-CTA" if chunk else "large-bucket", "gram_chunk": chunk or None}
-    g = lib.Graph(items)
+                    "kernel": "large-bucket" if big else "single-CTA",
+                    ("formation_chunk" if big else "gram_chunk"): shape}
+    claim = lib.multi_autotune(items)
+    g = lib.Graph(items, claim=claim)
     ms = timeit(g.launch, reps=2)
     bad = sum(int((it[4]["info"] != 0).sum().item()) for it in items)
     g.close()
     n = sum(it[1].shape[0] for it in items)
-    return {"cells": n, "ms": ms, "cells_per_s": n / ms * 1e3, "info_nonzero_cells": bad, "buckets": per}
+    return {"cells": n, "ms": ms, "cells_per_s": n / ms * 1e3, "info_nonzero_cells": bad, "queue_claim": claim,
+            "launches_per_assembly": 1, "buckets": per}
 
 
 def measured_hbm_gbs():

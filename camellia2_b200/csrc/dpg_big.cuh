@@ -27,7 +27,8 @@
 
 constexpr int ZT = 64;  // tile edge
 constexpr int ZL = 68;  // shared row stride, == 4 (mod 16) doubles: conflict-free DMMA fragments
-constexpr int ZK = 32;  // k-chunk of a formation tile (two m16n8k16 steps)
+// ZK (template parameter below): k-chunk of a formation tile, 16 or 32 points (one or two
+// m16n8k16 steps per chunk); the plan's big_zk, chosen by dpg_plan_autotune
 constexpr int BIG_NOFAIL = 0x7fffffff;
 
 struct BigSm {
@@ -36,7 +37,7 @@ struct BigSm {
   double* LI;  // [64][ZL] L panel rows of the current row block
   double* LJ;  // [64][ZL] panel rows of the column block / staging of the raw panel
   double* LJ1; // [64][ZL] second panel buffer (double buffering of the column blocks)
-  double* fa;  // [2][2][ZK][ZL] formation operands (rows, columns) x two chunks (aliases D)
+  double* fa;  // [2][2][ZK][ZL] formation operands (rows, columns) x two chunks (aliases D..LJ1)
   double* sc;  // [Np] equilibration scales
   int* col;    // [Np] test row record: var << 16 | local dof, or -1 (padding row)
   int* ints;   // [0] first failing G column, [1] first failing field column, [64..] relevance lists
@@ -62,6 +63,7 @@ __device__ __forceinline__ BigSm big_views(const DpgPlanDev& P) {
 // acc (a 16 x 16 warp tile: rows wr.., columns wc..) += A B over one ZK chunk, operands stored
 // k-major: A[r][k] = fa[k][r], B[k][c] = fb[k][c].  The k16 steps alternate between acc and
 // acc2, so four independent DMMA chains are in flight.
+template <int ZK>
 __device__ __forceinline__ void big_mma_kmajor(const double* fa, const double* fb, int wr, int wc, int g, int t,
                                                double (&acc)[2][4], double (&acc2)[2][4]) {
 #pragma unroll
@@ -182,6 +184,7 @@ __device__ void big_prep(const DpgPlanDev& P, const DpgLaunch& L, int cell, cons
 
 // One formation tile.  kind 0: G rows r0.., columns c0.. (test rows); kind 1: E^T rows
 // (device trial columns) r0.., columns c0.. (test rows).
+template <int ZK>
 __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind, int r0, int c0, bool diag, double* Z,
                               const BigSm& S, const double* wq, const double* bh, const double* vt) {
   (void)L;
@@ -295,7 +298,7 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
   for (int k0 = 0, c = 0; k0 < nk; k0 += ZK, c++) {
     // the products of chunk c are issued first, so they run while chunk c + 1's loads are in flight
     const double* fa = S.fa + (c & 1) * 2 * ZK * ZL;
-    big_mma_kmajor(fa, fa + ZK * ZL, wr, wc, g, t, acc, acc2);
+    big_mma_kmajor<ZK>(fa, fa + ZK * ZL, wr, wc, g, t, acc, acc2);
     if (k0 + ZK < nk) operands(k0 + ZK, (c + 1) & 1);
     __syncthreads();
   }
@@ -480,15 +483,9 @@ __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, con
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
-  const int tid = threadIdx.x;
-  const BigSm S = big_views(P);
-  double* const Z = L.scratch + (size_t)blockIdx.x * P.bz_per_cta;
-  double* const wq = Z + P.bz_wq;
-  double* const bh = Z + P.bz_bh;
-  double* const vt = Z + P.bz_vt;
-  const int Np = P.Np, Mp = P.Mp, M = P.M, ld = P.ldz;
-  for (int i = tid; i < Np; i += NT) {
+// Per-CTA table of a large plan: the test var and local dof of every device test row.
+__device__ __forceinline__ void big_cta_setup(const DpgPlanDev& P, const BigSm& S) {
+  for (int i = threadIdx.x; i < P.Np; i += NT) {
     int rec = -1;
     for (int a = 0; a < P.ntest; a++) {
       const int il = i - P.test[a].dev_off;
@@ -496,7 +493,17 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
     }
     S.col[i] = rec;
   }
-  for (int cell = blockIdx.x; cell < L.C; cell += gridDim.x) {
+}
+
+// One cell of a large plan; Z is this CTA's workspace (bz_per_cta doubles).
+template <int ZK>
+__device__ __forceinline__ void big_cell_body(const DpgPlanDev& P, const DpgLaunch& L, int cell, const BigSm& S, double* const Z) {
+  const int tid = threadIdx.x;
+  double* const wq = Z + P.bz_wq;
+  double* const bh = Z + P.bz_bh;
+  double* const vt = Z + P.bz_vt;
+  const int Np = P.Np, Mp = P.Mp, M = P.M, ld = P.ldz;
+  {
     __syncthreads();
     if (tid == 0) { S.ints[0] = BIG_NOFAIL; S.ints[1] = BIG_NOFAIL; }
     if (tid < P.nv * P.d) S.nodes[tid] = L.nodes[(size_t)cell * P.nv * P.d + tid];
@@ -508,11 +515,11 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
     }
     __syncthreads();
     const int nbg = (Np + ZT - 1) / ZT, nbm = (Mp + ZT - 1) / ZT;
-    for (int I = 0; I < nbg; I++) big_form_tile(P, L, 0, I * ZT, I * ZT, true, Z, S, wq, bh, vt);
+    for (int I = 0; I < nbg; I++) big_form_tile<ZK>(P, L, 0, I * ZT, I * ZT, true, Z, S, wq, bh, vt);
     for (int I = 1; I < nbg; I++)
-      for (int J = 0; J < I; J++) big_form_tile(P, L, 0, I * ZT, J * ZT, false, Z, S, wq, bh, vt);
+      for (int J = 0; J < I; J++) big_form_tile<ZK>(P, L, 0, I * ZT, J * ZT, false, Z, S, wq, bh, vt);
     for (int J = 0; J < nbm; J++)
-      for (int I = 0; I < nbg; I++) big_form_tile(P, L, 1, J * ZT, I * ZT, false, Z, S, wq, bh, vt);
+      for (int I = 0; I < nbg; I++) big_form_tile<ZK>(P, L, 1, J * ZT, I * ZT, false, Z, S, wq, bh, vt);
     if (L.parts) {
       // G (N, N), B (M, N) and F (N) in user numbering: Z unscaled (dpg_assemble_parts)
       __syncthreads();
@@ -535,7 +542,7 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
           L.F[(size_t)cell * N + us] = Z[(size_t)(Np + P.fcol) * ld + ds] / S.sc[ds];
         }
       __syncthreads();
-      continue;
+      return;
     }
     big_cholesky(P, Z, 0, Np, S, &S.ints[0]);
     if (L.energy) {
@@ -603,4 +610,12 @@ __global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ 
       L.info[cell] = v;
     }
   }
+}
+
+template <int ZK>
+__global__ void __launch_bounds__(NT, 1) dpg_big_kernel(const __grid_constant__ DpgPlanDev P, const DpgLaunch L) {
+  const BigSm S = big_views(P);
+  big_cta_setup(P, S);
+  for (int cell = blockIdx.x; cell < L.C; cell += gridDim.x)
+    big_cell_body<ZK>(P, L, cell, S, L.scratch + (size_t)blockIdx.x * P.bz_per_cta);
 }

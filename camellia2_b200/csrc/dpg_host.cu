@@ -582,6 +582,7 @@ static int big_layout(HostPlan* P) {
   g.bz_bh = (int)o; o += al((size_t)g.QGpad * g.niprows * g.ntest * 4);
   g.bz_vt = (int)o; o += al((size_t)vrow * 4);
   g.bz_per_cta = o;
+  g.big_zk = 32;
   int s = 5 * 64 * 68;  // diagonal block, its inverse, three panel blocks (formation buffers alias them)
   g.bs_sc = s; s += (g.Np + 15) & ~15;
   g.bs_col = s; s += ((g.Np + 1) / 2 + 15) & ~15;
@@ -1633,7 +1634,6 @@ int dpg_plan_autotune(dpg_plan* p, int C, const double* nodes, const int8_t* par
   if (!p) return fail(DPG_ERR_BAD_PLAN, "null plan");
   if (!chosen) return fail(DPG_ERR_INVALID_ARGUMENT, "null output");
   *chosen = 0;
-  if (p->hp.dev.big) return DPG_OK;  // the large-bucket kernel has one configuration
   if (C <= 0 || !nodes || !parity) return fail(DPG_ERR_INVALID_ARGUMENT, "cells, nodes and parity are required");
   if (p->hp.dev.nslots > 0 && !coeff) return fail(DPG_ERR_INVALID_ARGUMENT, "coefficients required by this plan");
   cudaStream_t st = (cudaStream_t)stream;
@@ -1654,9 +1654,12 @@ int dpg_plan_autotune(dpg_plan* p, int C, const double* nodes, const int8_t* par
   float best = -1.0f;
   DpgPlanDev best_plan = g0;
   int rc = DPG_OK;
-  for (int chg = DPG_CHG; chg >= DPG_CHG / 2 && rc == DPG_OK; chg /= 2) {
+  // candidates: single-CTA plans, the Gram staging chunk (8 or 4 points: the shared-memory
+  // layout and the kernel instance); large plans, the formation k-chunk (32 or 16 points)
+  for (int cnd = 0; cnd < 2 && rc == DPG_OK; cnd++) {
     DpgPlanDev cand = g0;
-    if (smem_layout(cand, chg, p->hp.adj_terms_ok) != DPG_OK) continue;
+    if (g0.big) cand.big_zk = cnd == 0 ? 32 : 16;
+    else if (smem_layout(cand, cnd == 0 ? DPG_CHG : DPG_CHG / 2, p->hp.adj_terms_ok) != DPG_OK) continue;
     if ((rc = dpg_configure_kernels(&cand)) != DPG_OK) break;
     if ((rc = dpg_launch_assemble(&cand, nullptr, &L, st)) != DPG_OK) break;  // warm-up
     cudaEventRecord(e0, st);
@@ -1680,7 +1683,7 @@ int dpg_plan_autotune(dpg_plan* p, int C, const double* nodes, const int8_t* par
     return fail(DPG_ERR_CUDA, "plan upload");
   rc = dpg_configure_kernels(&p->hp.dev);
   if (rc != DPG_OK) return rc;
-  *chosen = p->hp.dev.chg;
+  *chosen = p->hp.dev.big ? p->hp.dev.big_zk : p->hp.dev.chg;
   return DPG_OK;
 }
 
@@ -1847,18 +1850,29 @@ int dpg_recover_fields(dpg_plan* p, int C, const double* K, const double* l, con
 // The buckets of a multi-bucket call: the single-CTA ones stay in (plans, ls) for one
 // persistent launch; the large ones move to (bp, bl) and follow on the same stream, one
 // launch of the large-bucket kernel each.
+// Work items a CTA of the multi-bucket launch claims at a time (flags bits 8-15; 0 -> 1).
+static int claim_of(int flags) { return std::max(1, (flags >> 8) & 0xff); }
+
+// The large buckets go to their own launches (the specialized kernel, whose plan lives in
+// kernel parameters: a work queue holding them ran their cells 11-28 % slower), in
+// decreasing order of per-cell cost; the single-CTA buckets share one work-queue launch.
 static void split_big(std::vector<DpgPlanDev>& plans, std::vector<DpgLaunch>& ls, std::vector<DpgPlanDev>& bp,
                       std::vector<DpgLaunch>& bl) {
   std::vector<DpgPlanDev> sp;
   std::vector<DpgLaunch> sl;
+  std::vector<size_t> big;
   for (size_t i = 0; i < plans.size(); i++) {
     if (plans[i].big) {
-      bp.push_back(plans[i]);
-      bl.push_back(ls[i]);
+      big.push_back(i);
     } else {
       sp.push_back(plans[i]);
       sl.push_back(ls[i]);
     }
+  }
+  std::stable_sort(big.begin(), big.end(), [&](size_t x, size_t y) { return plans[x].Zn > plans[y].Zn; });
+  for (size_t i : big) {
+    bp.push_back(plans[i]);
+    bl.push_back(ls[i]);
   }
   plans.swap(sp);
   ls.swap(sl);
@@ -1870,10 +1884,53 @@ int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* str
   int rc = multi_args(n_buckets, buckets, flags, plans, ls);
   if (rc != DPG_OK) return rc;
   split_big(plans, ls, bp, bl);
-  if (!plans.empty()) rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), (cudaStream_t)stream, nullptr);
   for (size_t i = 0; rc == DPG_OK && i < bp.size(); i++)
-    if (bl[i].C > 0) rc = dpg_launch_assemble(&bp[i], nullptr, &bl[i], (cudaStream_t)stream);
+    rc = dpg_launch_assemble(&bp[i], nullptr, &bl[i], (cudaStream_t)stream);
+  if (rc == DPG_OK && !plans.empty())
+    rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), (cudaStream_t)stream, nullptr, claim_of(flags));
   return rc;
+}
+
+int dpg_multi_autotune(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags, int* chosen) {
+  if (!chosen) return fail(DPG_ERR_INVALID_ARGUMENT, "null output");
+  *chosen = 0;
+  std::vector<DpgPlanDev> plans, bp;
+  std::vector<DpgLaunch> ls, bl;
+  int rc = multi_args(n_buckets, buckets, flags, plans, ls);
+  if (rc != DPG_OK) return rc;
+  split_big(plans, ls, bp, bl);  // the claim size concerns the work queue of the single-CTA buckets
+  if (plans.empty()) {
+    *chosen = 1;
+    return DPG_OK;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = -1.0f;
+  int best_claim = 1;
+  for (int claim : {1, 2, 4, 8}) {
+    if ((rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), st, nullptr, claim)) != DPG_OK) break;
+    cudaEventRecord(e0, st);
+    rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), st, nullptr, claim);
+    cudaEventRecord(e1, st);
+    if (rc != DPG_OK) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = fail(DPG_ERR_CUDA, "multi autotune timing");
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (best < 0.0f || ms < best) {
+      best = ms;
+      best_claim = claim;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != DPG_OK) return rc;
+  *chosen = best_claim;
+  return DPG_OK;
 }
 
 struct dpg_graph {
@@ -1893,9 +1950,8 @@ int dpg_graph_capture(int n_buckets, const dpg_bucket_batch* buckets, int flags,
   if (rc != DPG_OK) return rc;
   split_big(plans, ls, bp, bl);
   size_t big_bytes = 0;
-  for (size_t i = 0; i < bp.size(); i++)
-    if (bl[i].C > 0) big_bytes = std::max(big_bytes, dpg_big_workspace_bytes(&bp[i], bl[i].C));
-  if (plans.empty() && big_bytes == 0) return fail(DPG_ERR_INVALID_ARGUMENT, "no cells to capture");
+  for (size_t i = 0; i < bp.size(); i++) big_bytes = std::max(big_bytes, dpg_big_workspace_bytes(&bp[i], bl[i].C));
+  if (plans.empty() && bp.empty()) return fail(DPG_ERR_INVALID_ARGUMENT, "no cells to capture");
   dpg_graph* G = new dpg_graph();
   std::memset(&G->dev, 0, sizeof(G->dev));
   cudaGetDevice(&G->device);
@@ -1903,29 +1959,33 @@ int dpg_graph_capture(int n_buckets, const dpg_bucket_batch* buckets, int flags,
     G->dev.bytes = dpg_multi_bytes(plans.data(), ls.data(), (int)plans.size());
     if (cudaMalloc(&G->dev.base, G->dev.bytes) != cudaSuccess) {
       cudaGetLastError();
-      delete G;
+      G->dev.base = nullptr;
+      dpg_graph_destroy(G);
       return fail(DPG_ERR_OUT_OF_MEMORY, "graph workspace");
     }
-    rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), nullptr, &G->dev);
+    rc = dpg_launch_multi(plans.data(), ls.data(), (int)plans.size(), nullptr, &G->dev, claim_of(flags));
   }
   if (rc == DPG_OK && big_bytes > 0 && cudaMalloc(&G->big_ws, big_bytes) != cudaSuccess) {
     cudaGetLastError();
     G->big_ws = nullptr;
     rc = fail(DPG_ERR_OUT_OF_MEMORY, "graph workspace of the large buckets");
   }
-  cudaStream_t cs = nullptr;
-  if (rc == DPG_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+  // one stream: the large buckets' launches in decreasing order of cost, then the work queue
+  // of the single-CTA buckets (run beside them on a second branch, the queue's CTAs took SMs
+  // before the long large cells had started and lengthened the whole: 1.19 s against 1.17 s
+  // on the uneven-cell workload)
+  cudaStream_t cs0 = nullptr;
+  if (rc == DPG_OK && cudaStreamCreateWithFlags(&cs0, cudaStreamNonBlocking) != cudaSuccess)
     rc = fail(DPG_ERR_CUDA, "stream creation");
   if (rc == DPG_OK) {
-    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    cudaError_t e = cudaStreamBeginCapture(cs0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      if (!plans.empty()) rc = dpg_launch_multi_prepared(&G->dev, cs);
       for (size_t i = 0; rc == DPG_OK && i < bp.size(); i++) {
-        if (bl[i].C <= 0) continue;
         bl[i].scratch = (double*)G->big_ws;
-        rc = dpg_launch_assemble(&bp[i], nullptr, &bl[i], cs);
+        rc = dpg_launch_assemble(&bp[i], nullptr, &bl[i], cs0);
       }
-      cudaError_t e2 = cudaStreamEndCapture(cs, &G->graph);
+      if (rc == DPG_OK && !plans.empty()) rc = dpg_launch_multi_prepared(&G->dev, cs0);
+      cudaError_t e2 = cudaStreamEndCapture(cs0, &G->graph);
       if (rc == DPG_OK && e2 != cudaSuccess) rc = fail(DPG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e2));
     } else {
       rc = fail(DPG_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
@@ -1933,7 +1993,7 @@ int dpg_graph_capture(int n_buckets, const dpg_bucket_batch* buckets, int flags,
   }
   if (rc == DPG_OK && cudaGraphInstantiate(&G->exec, G->graph, 0) != cudaSuccess)
     rc = fail(DPG_ERR_CUDA, "graph instantiation");
-  if (cs) cudaStreamDestroy(cs);
+  if (cs0) cudaStreamDestroy(cs0);
   if (rc != DPG_OK) {
     cudaGetLastError();
     dpg_graph_destroy(G);

@@ -68,17 +68,20 @@ int dpg_launch_scatter_global(int C, int t, const int64_t* ptr, const int64_t* g
 int dpg_launch_recover_fields(int C, int M, int nf, const double* K, const double* l, const double* t, double* u,
                               int32_t* info, cudaStream_t stream);
 
-// Device tables of a prepared multi-bucket launch (CUDA graph capture).
+// Device tables of a prepared work-queue launch of single-CTA buckets (CUDA graph capture).
 struct DpgMultiDev {
-  void* base;          // caller-owned device block: tables, then scratch
+  void* base;          // caller-owned device block: tables, counters, then scratch slots
   size_t bytes;
   DpgPlanDev* plans;
   DpgLaunch* launches;
   int* cstart;
+  int* counters;       // claim and leave counters (the kernel resets them at its end)
   int nb, grid;
+  int claim, claim_slot;
   void* kernel;
   size_t smem;
 };
-int dpg_launch_multi(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb, cudaStream_t stream, DpgMultiDev* dev);
+int dpg_launch_multi(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb, cudaStream_t stream, DpgMultiDev* dev,
+                     int claim);
 int dpg_launch_multi_prepared(const DpgMultiDev* dev, cudaStream_t stream);
 size_t dpg_multi_bytes(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb);

@@ -1175,75 +1175,108 @@ __device__ __forceinline__ void cta_setup(const DpgPlanDev& P) {
   __syncthreads();
 }
 
-// Several buckets in one persistent launch.  Work item i of the concatenated cell
-// ranges (bucket b owns [cstart[b], cstart[b+1])) goes to CTA i mod grid, so every
-// CTA walks the buckets in order and switches tables at most nb - 1 times.  The
-// plans live in global memory; their scratch strides are the launch's common one.
+#include "dpg_energy.cuh"
+#include "dpg_big.cuh"
+
+
+// Claim `claim` work items from the queue counter; all threads see the same base.
+__device__ __forceinline__ int queue_claim(int* counter, int claim, volatile int* slot) {
+  if (threadIdx.x == 0) *slot = atomicAdd(counter, claim);
+  __syncthreads();
+  const int base = *slot;
+  __syncthreads();  // every thread has its copy before the next claim overwrites it
+  return base;
+}
+
+// The last CTA to leave the queue resets its counters, so the next launch (a graph
+// replay) starts from zero; no CTA waits on another.
+__device__ __forceinline__ void queue_leave(int* counters) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&counters[1], 1) == (int)gridDim.x - 1) {
+      counters[0] = 0;
+      counters[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
+// Multi-bucket work queue of the single-CTA plans: the buckets' cell ranges are
+// concatenated in decreasing order of per-cell cost (the host orders them), and each CTA
+// claims `claim` consecutive cells at a time from a device counter, so the long cells start
+// first and the short ones fill the tail.  Switching buckets rebuilds the CTA's tables and
+// mbarriers.  claim_slot: a shared-memory double beyond every plan's layout.
 template <int NBTM, int GTM, int BTW>
-__global__ void __launch_bounds__(NT, 1) dpg_multi_kernel(const DpgPlanDev* __restrict__ plans,
+__global__ void __launch_bounds__(NT, 1) dpg_queue_kernel(const DpgPlanDev* __restrict__ plans,
                                                           const DpgLaunch* __restrict__ launches,
-                                                          const int* __restrict__ cstart, int nb) {
+                                                          const int* __restrict__ cstart, int nb,
+                                                          int* __restrict__ counters, int claim, int claim_slot) {
   const int tid = threadIdx.x;
   Ctx X;
   uint32_t phase[4] = {0, 0, 0, 0};
   X.phase = phase;
   double* const sm = dpg_smem;
+  volatile int* const claim_s = reinterpret_cast<volatile int*>(sm + claim_slot);
   int cur = -1;
   const int total = cstart[nb];
-  for (int i = blockIdx.x; i < total; i += gridDim.x) {
-    int b = cur < 0 ? 0 : cur;
-    while (i >= cstart[b + 1]) b++;
-    const DpgPlanDev& P = plans[b];
-    const DpgLaunch& L = launches[b];
-    if (b != cur) {
+  for (;;) {
+    const int base = queue_claim(&counters[0], claim, claim_s);
+    if (base >= total) break;
+    const int end = min(total, base + claim);
+    for (int i = base; i < end; i++) {
+      int b = cur < 0 ? 0 : cur;
+      while (i >= cstart[b + 1]) b++;
+      const DpgPlanDev& P = plans[b];
+      const DpgLaunch& L = launches[b];
+      if (b != cur) {
+        __syncthreads();
+        if (cur >= 0 && tid == 0) {
+          uint64_t* old = reinterpret_cast<uint64_t*>(sm + plans[cur].sm_nodes + 26);
+          for (int k = 0; k < 4; k++) mbar_inval(&old[k]);
+        }
+        __syncthreads();
+        cta_setup(P);
+        for (int k = 0; k < 4; k++) phase[k] = 0;
+        cur = b;
+      }
+      const int cell = i - cstart[b];
+      double* nodes_s = sm + P.sm_nodes;
+      int* flag_s = reinterpret_cast<int*>(sm + P.sm_nodes + 24);
+      double* coef_s = sm + P.sm_coef;
+      if (tid == 0) { flag_s[0] = 0; flag_s[1] = 0; flag_s[2] = 0; }
+      if (tid < P.nv * P.d) nodes_s[tid] = L.nodes[(size_t)cell * P.nv * P.d + tid];
+      const int nco = P.nslots * P.Ptot;
+      if (L.coeff)
+        for (int k = tid; k < nco; k += NT) coef_s[k] = L.coeff[(size_t)cell * nco + k];
       __syncthreads();
-      if (cur >= 0 && tid == 0) {
-        uint64_t* old = reinterpret_cast<uint64_t*>(sm + plans[cur].sm_nodes + 26);
-        for (int k = 0; k < 4; k++) mbar_inval(&old[k]);
+      phase_b<BTW>(P, L, cell, X);
+      __syncthreads();
+      phase_gram<GTM, 0>(P, L, cell, X);
+      phase_factor(P, X);
+      phase_trsm<NBTM>(P, L, cell, X);
+      phase_syrk_out(P, L, cell, X);
+      __syncthreads();
+      if (tid == 0 && L.info) {
+        int v = 0;
+        if (flag_s[2]) v = ERR_TIMEOUT_FLAG;
+        else if (flag_s[0] != 0) {
+          int r = flag_s[0] - 1;
+          int u = P.dev2user_test[r];
+          v = (u >= 0 ? u : r) + 1;
+        } else if (flag_s[1] != 0) v = flag_s[1];
+        L.info[cell] = v;
       }
       __syncthreads();
-      cta_setup(P);
-      for (int k = 0; k < 4; k++) phase[k] = 0;
-      cur = b;
     }
-    const int cell = i - cstart[b];
-    double* nodes_s = sm + P.sm_nodes;
-    int* flag_s = reinterpret_cast<int*>(sm + P.sm_nodes + 24);
-    double* coef_s = sm + P.sm_coef;
-    if (tid == 0) { flag_s[0] = 0; flag_s[1] = 0; flag_s[2] = 0; }
-    if (tid < P.nv * P.d) nodes_s[tid] = L.nodes[(size_t)cell * P.nv * P.d + tid];
-    const int nco = P.nslots * P.Ptot;
-    if (L.coeff)
-      for (int k = tid; k < nco; k += NT) coef_s[k] = L.coeff[(size_t)cell * nco + k];
-    __syncthreads();
-    phase_b<BTW>(P, L, cell, X);
-    __syncthreads();
-    phase_gram<GTM, 0>(P, L, cell, X);
-    phase_factor(P, X);
-    phase_trsm<NBTM>(P, L, cell, X);
-    phase_syrk_out(P, L, cell, X);
-    __syncthreads();
-    if (tid == 0 && L.info) {
-      int v = 0;
-      if (flag_s[2]) v = ERR_TIMEOUT_FLAG;
-      else if (flag_s[0] != 0) {
-        int r = flag_s[0] - 1;
-        int u = P.dev2user_test[r];
-        v = (u >= 0 ? u : r) + 1;
-      } else if (flag_s[1] != 0) v = flag_s[1];
-      L.info[cell] = v;
-    }
-    __syncthreads();
   }
+  queue_leave(counters);
 }
 
-#include "dpg_energy.cuh"
-#include "dpg_big.cuh"
+typedef void (*QueueFn)(const DpgPlanDev*, const DpgLaunch*, const int*, int, int*, int, int);
+#define DPG_QUEUE_INSTANCES(X) X(16, 6, 4) X(24, 12, 6)
 
-typedef void (*MultiFn)(const DpgPlanDev*, const DpgLaunch*, const int*, int);
-#define DPG_MULTI_INSTANCES(X) X(16, 6, 4) X(24, 12, 6)
-
-static MultiFn pick_multi_kernel(const DpgPlanDev* plans, int nb) {
+// The smallest instance whose register arrays cover every single-CTA plan of the call.
+static QueueFn pick_queue_kernel(const DpgPlanDev* plans, int nb) {
   int nbt = 0, per = 0, btw = 0;
   for (int b = 0; b < nb; b++) {
     const DpgPlanDev* p = &plans[b];
@@ -1252,8 +1285,8 @@ static MultiFn pick_multi_kernel(const DpgPlanDev* plans, int nb) {
     for (int s = 0; s < p->nseg; s++) btw = std::max(btw, (p->seg[s].ntile + DPG_NWARPS - 1) / DPG_NWARPS);
   }
 #define DPG_PICK(NB, GT, BT) \
-  if (nbt <= NB && per <= GT && btw <= BT) return dpg_multi_kernel<NB, GT, BT>;
-  DPG_MULTI_INSTANCES(DPG_PICK)
+  if (nbt <= NB && per <= GT && btw <= BT) return dpg_queue_kernel<NB, GT, BT>;
+  DPG_QUEUE_INSTANCES(DPG_PICK)
 #undef DPG_PICK
   return nullptr;
 }
@@ -1325,8 +1358,10 @@ static int configure_big(const DpgPlanDev* plan) {
   // every large plan shares the kernel: opt in to the device maximum so that configuring one
   // plan never lowers the limit another plan needs
   if (optin > 0) bytes = (size_t)optin;
-  cudaError_t e = cudaFuncSetAttribute(dpg_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  for (KernelFn k : {dpg_big_kernel<16>, dpg_big_kernel<32>}) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  }
   return DPG_OK;
 }
 
@@ -1345,7 +1380,8 @@ static int launch_big(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t
     }
     L.scratch = (double*)ws;
   }
-  dpg_big_kernel<<<grid, NT, (size_t)plan->bs_total * sizeof(double), stream>>>(*plan, L);
+  KernelFn k = plan->big_zk == 16 ? dpg_big_kernel<16> : dpg_big_kernel<32>;
+  k<<<grid, NT, (size_t)plan->bs_total * sizeof(double), stream>>>(*plan, L);
   cudaError_t e = cudaGetLastError();
   if (ws) cudaFreeAsync(ws, stream);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
@@ -1724,89 +1760,124 @@ int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t
   return DPG_OK;
 }
 
-// hplans: host copies of the buckets' plans (their scratch_per_cta is replaced by
-// the common stride here); hl: per-bucket launch arguments; dev: where the device
-// copies of the tables go (null: stream-ordered temporaries freed after the launch).
-int dpg_launch_multi(const DpgPlanDev* hplans_in, const DpgLaunch* hl_in, int nb, cudaStream_t stream,
-                     DpgMultiDev* dev) {
-  std::vector<DpgPlanDev> hplans(hplans_in, hplans_in + nb);
-  std::vector<DpgLaunch> hl(hl_in, hl_in + nb);
-  std::vector<int> cstart(nb + 1, 0);
-  size_t stride = 0, smem = 0;
+// The work queue of the single-CTA plans: the buckets that have cells, in decreasing order of
+// per-cell cost (the cube of the order of the matrix a cell factors), their concatenated
+// cell ranges, the common per-CTA scratch stride, the shared memory of the largest plan plus
+// the claim slot, and the device bytes: tables, two counters, scratch slots.
+struct QueuePart {
+  std::vector<DpgPlanDev> plans;
+  std::vector<DpgLaunch> ls;
+  std::vector<int> cstart{0};
+  size_t stride = 0;
+  int smem_doubles = 0, claim_slot = 0;
+  int total = 0, grid = 0;
+  size_t bytes_tables = 0, bytes = 0;
+};
+
+static int queue_part(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb, QueuePart& Q) {
+  std::vector<int> order;
   for (int b = 0; b < nb; b++) {
-    if (hplans[b].big && hl[b].C > 0)
-      return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans run through dpg_assemble, not the multi-bucket launch");
-    cstart[b + 1] = cstart[b] + std::max(0, hl[b].C);
-    stride = std::max(stride, hplans[b].scratch_per_cta);
-    smem = std::max(smem, (size_t)hplans[b].sm_total * sizeof(double));
+    if (hl[b].C <= 0) continue;
+    if (hplans[b].big) return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans run on their own launches");
+    if (hl[b].solve_only) return dpg::fail(DPG_ERR_UNSUPPORTED, "the multi-bucket launch assembles; no solve-only plans");
+    order.push_back(b);
   }
-  const int total = cstart[nb];
-  if (total == 0) return DPG_OK;
-  MultiFn k = pick_multi_kernel(hplans.data(), nb);
+  auto cost = [&](int b) {
+    const double n = (double)(hplans[b].Np + hplans[b].Mp);
+    return n * n * n;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+  for (int b : order) {
+    Q.stride = std::max(Q.stride, hplans[b].scratch_per_cta);
+    Q.smem_doubles = std::max(Q.smem_doubles, hplans[b].sm_total);
+    Q.plans.push_back(hplans[b]);
+    Q.ls.push_back(hl[b]);
+    Q.cstart.push_back(Q.cstart.back() + hl[b].C);
+  }
+  Q.total = Q.cstart.back();
+  Q.grid = std::min(std::max(Q.total, 1), dpg::num_sms());
+  for (auto& p : Q.plans) p.scratch_per_cta = Q.stride;
+  Q.claim_slot = (Q.smem_doubles + 1) & ~1;
+  const int nq = (int)Q.plans.size();
+  Q.bytes_tables = (nq * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)) + (nq + 1) * sizeof(int) + 8 + 255) & ~(size_t)255;
+  Q.bytes = Q.bytes_tables + (size_t)Q.grid * Q.stride * sizeof(double);
+  return DPG_OK;
+}
+
+// hplans: host copies of the single-CTA buckets' plans; hl: per-bucket launch arguments;
+// claim: cells a CTA claims at a time; dev: where the device copies of the tables go (null:
+// stream-ordered temporaries freed after the launch).
+int dpg_launch_multi(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb, cudaStream_t stream, DpgMultiDev* dev,
+                     int claim) {
+  QueuePart Q;
+  int rc = queue_part(hplans, hl, nb, Q);
+  if (rc != DPG_OK) return rc;
+  if (Q.total == 0) return DPG_OK;
+  const int nq = (int)Q.plans.size();
+  QueueFn k = pick_queue_kernel(Q.plans.data(), nq);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no multi-bucket kernel instance covers these buckets");
   int dev_id = 0, optin = 0;
   cudaGetDevice(&dev_id);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev_id);
+  const size_t smem = (size_t)(Q.claim_slot + 2) * sizeof(double);
+  if (optin > 0 && smem > (size_t)optin)
+    return dpg::fail(DPG_ERR_UNSUPPORTED, "multi-bucket launch: no room for the claim slot beside the largest plan");
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin > 0 ? optin : (int)smem);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-  const int grid = std::min(total, dpg::num_sms());
-  for (auto& p : hplans) p.scratch_per_cta = stride;
-  const size_t bytes_tables = nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)) + (nb + 1) * sizeof(int) + 256;
-  const size_t bytes_scratch = (size_t)grid * stride * sizeof(double);
+  claim = std::max(1, std::min(claim, 64));
   char* base = nullptr;
   if (dev) {
-    if (dev->bytes < bytes_tables + bytes_scratch) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "multi workspace too small");
+    if (dev->bytes < Q.bytes) return dpg::fail(DPG_ERR_INVALID_ARGUMENT, "multi workspace too small");
     base = (char*)dev->base;
   } else {
-    e = dpg::ws_alloc((void**)&base, bytes_tables + bytes_scratch, stream);
+    e = dpg::ws_alloc((void**)&base, Q.bytes, stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return dpg::fail(DPG_ERR_OUT_OF_MEMORY, std::string("multi workspace: ") + cudaGetErrorString(e));
     }
   }
-  double* scratch = (double*)(base + ((bytes_tables + 255) & ~(size_t)255));
-  for (auto& l : hl) l.scratch = scratch;
+  double* scratch = (double*)(base + Q.bytes_tables);
+  for (auto& l : Q.ls) l.scratch = scratch;
   DpgPlanDev* d_plans = (DpgPlanDev*)base;
-  DpgLaunch* d_l = (DpgLaunch*)(base + nb * sizeof(DpgPlanDev));
-  int* d_cs = (int*)(base + nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)));
-  if (dev) {  // outside any capture: synchronous uploads
-    cudaMemcpy(d_plans, hplans.data(), nb * sizeof(DpgPlanDev), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_l, hl.data(), nb * sizeof(DpgLaunch), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_cs, cstart.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice);
-    dev->plans = d_plans; dev->launches = d_l; dev->cstart = d_cs; dev->nb = nb; dev->grid = grid;
-    dev->kernel = (void*)k; dev->smem = smem;
+  DpgLaunch* d_l = (DpgLaunch*)(base + nq * sizeof(DpgPlanDev));
+  int* d_cs = (int*)(base + nq * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)));
+  int* d_ctr = d_cs + nq + 1;
+  if (dev) {  // outside any capture: synchronous uploads; the kernel resets its counters itself
+    cudaMemcpy(d_plans, Q.plans.data(), nq * sizeof(DpgPlanDev), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_l, Q.ls.data(), nq * sizeof(DpgLaunch), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_cs, Q.cstart.data(), (nq + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    e = cudaMemset(d_ctr, 0, 2 * sizeof(int));
+    if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("counter reset: ") + cudaGetErrorString(e));
+    dev->plans = d_plans; dev->launches = d_l; dev->cstart = d_cs; dev->nb = nq; dev->grid = Q.grid;
+    dev->kernel = (void*)k; dev->smem = smem; dev->counters = d_ctr; dev->claim = claim; dev->claim_slot = Q.claim_slot;
     return DPG_OK;
   }
-  cudaMemcpyAsync(d_plans, hplans.data(), nb * sizeof(DpgPlanDev), cudaMemcpyHostToDevice, stream);
-  cudaMemcpyAsync(d_l, hl.data(), nb * sizeof(DpgLaunch), cudaMemcpyHostToDevice, stream);
-  cudaMemcpyAsync(d_cs, cstart.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, stream);
-  k<<<grid, NT, smem, stream>>>(d_plans, d_l, d_cs, nb);
+  cudaMemcpyAsync(d_plans, Q.plans.data(), nq * sizeof(DpgPlanDev), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_l, Q.ls.data(), nq * sizeof(DpgLaunch), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_cs, Q.cstart.data(), (nq + 1) * sizeof(int), cudaMemcpyHostToDevice, stream);
+  cudaMemsetAsync(d_ctr, 0, 2 * sizeof(int), stream);
+  k<<<Q.grid, NT, smem, stream>>>(d_plans, d_l, d_cs, nq, d_ctr, claim, Q.claim_slot);
   e = cudaGetLastError();
   cudaFreeAsync(base, stream);
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
 }
 
-// Launch of tables prepared by dpg_launch_multi(..., dev) (graph capture records this).
+// Launch of the queue prepared by dpg_launch_multi(..., dev) (graph capture records this).
 int dpg_launch_multi_prepared(const DpgMultiDev* dev, cudaStream_t stream) {
-  MultiFn k = (MultiFn)dev->kernel;
-  k<<<dev->grid, NT, dev->smem, stream>>>(dev->plans, dev->launches, dev->cstart, dev->nb);
+  QueueFn k = (QueueFn)dev->kernel;
+  k<<<dev->grid, NT, dev->smem, stream>>>(dev->plans, dev->launches, dev->cstart, dev->nb, dev->counters, dev->claim,
+                                          dev->claim_slot);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return dpg::fail(DPG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return DPG_OK;
 }
 
-// Bytes a prepared multi-bucket launch needs (tables + scratch).
+// Bytes a prepared multi-bucket launch needs (tables, counters, scratch slots).
 size_t dpg_multi_bytes(const DpgPlanDev* hplans, const DpgLaunch* hl, int nb) {
-  size_t stride = 0;
-  int total = 0;
-  for (int b = 0; b < nb; b++) {
-    stride = std::max(stride, hplans[b].scratch_per_cta);
-    total += std::max(0, hl[b].C);
-  }
-  const int grid = std::min(std::max(total, 1), dpg::num_sms());
-  const size_t tables = nb * (sizeof(DpgPlanDev) + sizeof(DpgLaunch)) + (nb + 1) * sizeof(int) + 256;
-  return ((tables + 255) & ~(size_t)255) + (size_t)grid * stride * sizeof(double);
+  QueuePart Q;
+  if (queue_part(hplans, hl, nb, Q) != DPG_OK) return 0;
+  return Q.bytes;
 }
 
 // ---------------------------------------------------------------------------

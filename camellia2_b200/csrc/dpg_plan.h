@@ -214,6 +214,7 @@ struct DpgPlanDev {
   int bz_wq, bz_bh, bz_vt;  // per-CTA workspace after Z: w|J| at Gram points, per-point IP row
                             // factors [QG][rows][ntest][4], per-point term factors [vt rows][4]
   size_t bz_per_cta;        // doubles of per-CTA workspace
+  int big_zk;               // formation k-chunk (16 or 32 points; dpg_plan_autotune picks it)
   int bs_sc, bs_col, bs_int, bs_nodes, bs_total;  // shared memory (doubles): scales, column
                                                   // records, ints, vertices; total
 };

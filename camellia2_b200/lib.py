@@ -53,6 +53,7 @@ def load():
     L.dpg_factored_cholesky_solve.argtypes = [i, i, i] + [vp] * 6 + [vp]
     L.dpg_assemble_adjoint.argtypes = [vp, i] + [vp] * 7 + [vp]
     L.dpg_assemble_multi.argtypes = [i, vp, vp, i]
+    L.dpg_multi_autotune.argtypes = [i, vp, vp, i, ct.POINTER(i)]
     L.dpg_recover_fields.argtypes = [vp, i] + [vp] * 5 + [vp]
     L.dpg_energy_error.argtypes = [vp, i] + [vp] * 6 + [vp]
     L.dpg_assemble_dls.argtypes = [vp, i] + [vp] * 6 + [vp]
@@ -141,8 +142,9 @@ class Plan:
         return o["K"], o["l"]
 
     def autotune(self, nodes, parity, coeff=None, stream=None):
-        """dpg_plan_autotune: time the Gram staging chunk sizes that fit on these cells (device
-        tensors) and keep the faster; returns the chosen chunk (0 for a large-bucket plan)."""
+        """dpg_plan_autotune: time the candidate shapes on these cells (device tensors) and keep
+        the faster; returns the chosen Gram staging chunk (single-CTA plans: 8 or 4) or the
+        formation k-chunk (large-bucket plans: 32 or 16)."""
         chosen = ct.c_int(0)
         _check(load().dpg_plan_autotune(self.h, nodes.shape[0], _ptr(nodes), _ptr(parity), _ptr(coeff),
                                         _stream_ptr(stream), ct.byref(chosen)))
@@ -256,19 +258,32 @@ def _batches(items):
     return arr
 
 
-def assemble_multi(items, stream=None, flags=0):
-    """dpg_assemble_multi: several buckets in one call; the single-CTA buckets share one
-    persistent launch, the large buckets follow on the same stream."""
+def assemble_multi(items, stream=None, flags=0, claim=None):
+    """dpg_assemble_multi: several buckets, single-CTA and large, in one persistent launch with a
+    dynamic work queue; `claim` cells are taken from the queue at a time (flags bits 8-15)."""
     arr = _batches(items)
+    if claim is not None:
+        flags = (flags & 0xff) | ((int(claim) & 0xff) << 8)
     _check(load().dpg_assemble_multi(len(items), ct.cast(arr, ct.c_void_p), _stream_ptr(stream), flags))
+
+
+def multi_autotune(items, stream=None, flags=0):
+    """dpg_multi_autotune: the fastest claim size (cells per queue claim) for these buckets."""
+    arr = _batches(items)
+    chosen = ct.c_int(0)
+    _check(load().dpg_multi_autotune(len(items), ct.cast(arr, ct.c_void_p), _stream_ptr(stream), flags,
+                                     ct.byref(chosen)))
+    return chosen.value
 
 
 class Graph:
     """dpg_graph_capture / dpg_graph_launch: a captured multi-bucket launch replayed on
     the buffers named at capture time."""
 
-    def __init__(self, items, flags=0):
+    def __init__(self, items, flags=0, claim=None):
         self._keep = items  # the buffers must outlive the graph
+        if claim is not None:
+            flags = (flags & 0xff) | ((int(claim) & 0xff) << 8)
         arr = _batches(items)
         h = ct.c_void_p()
         _check(load().dpg_graph_capture(len(items), ct.cast(arr, ct.c_void_p), flags, ct.byref(h)))

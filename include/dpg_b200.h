@@ -113,6 +113,8 @@ extern "C" {
 /* dpg_assemble flags */
 #define DPG_FLAG_NO_K 1        /* do not write K / l (condensed outputs only) */
 #define DPG_FLAG_NO_CONDENSE 2 /* do not write S / s */
+/* multi-bucket calls: cells a CTA claims from the work queue at a time (1..255) */
+#define DPG_FLAG_CLAIM(n) (((n) & 0xff) << 8)
 
 typedef struct dpg_var_desc {
   int kind;       /* DPG_VAR_* */
@@ -203,13 +205,14 @@ int dpg_plan_query(const dpg_plan* plan, dpg_plan_info* info);
 
 /* Per-bucket autotuner (no counterpart in the reference: Camellia has no GPU
  * launch shapes to choose).  Times dpg_assemble on the C given cells (DEVICE
- * pointers as for dpg_assemble) with each Gram staging chunk that fits the
- * bucket's shared memory (8 and 4 quadrature points per chunk: the chunk sets
- * the shared-memory layout and the kernel instance), keeps the faster for all
- * later calls on this plan and returns its chunk size in *chosen (0 for a
- * large-bucket plan, which has a single configuration).  Results of the two
- * configurations agree to rounding (the Gram sums are ordered differently).
- * Allocates its timing outputs from the stream-ordered pool. */
+ * pointers as for dpg_assemble) with each candidate shape, keeps the faster for
+ * all later calls on this plan (dpg_assemble, the multi-bucket launch and its
+ * graph) and returns it in *chosen: for single-CTA plans the Gram staging chunk
+ * that fits the bucket's shared memory (8 or 4 quadrature points per chunk: it
+ * sets the shared-memory layout and the kernel instance), for large-bucket plans
+ * the formation k-chunk (32 or 16 points).  Results of the configurations agree
+ * to rounding (sums are ordered differently).  Allocates its timing outputs from
+ * the library's pool. */
 int dpg_plan_autotune(dpg_plan* plan, int C, const double* nodes, const int8_t* parity, const double* coeff,
                       void* stream, int* chosen);
 
@@ -337,9 +340,15 @@ int dpg_compose_map(int C, int t, const int64_t* map_ptr, const int64_t* map_gid
                     int64_t* out_count, int* missing, void* stream);
 
 /* Multi-bucket assembly (TSolution::populateStiffnessAndLoad's loop over
- * ElementType buckets, Solution.cpp:1131-1297): one persistent launch walks the
- * concatenated cell ranges of several plans. Pointers per bucket as in
- * dpg_assemble (device memory). */
+ * ElementType buckets, Solution.cpp:1131-1297).  The single-CTA buckets share one
+ * persistent work-queue launch: their cell ranges are concatenated in decreasing
+ * order of per-cell cost and each CTA claims DPG_FLAG_CLAIM(n) cells at a time
+ * (default 1) from a device counter, so long cells start first and short ones fill
+ * the tail; no CTA waits on another.  Each large bucket runs its own persistent
+ * launch, in decreasing order of cost (a queue holding large cells ran them 11-28 %
+ * slower: the specialized kernel keeps its plan in parameter space and a register
+ * allocation of its own).  Pointers per bucket as in dpg_assemble (device memory);
+ * flags as for dpg_assemble plus the claim size. */
 typedef struct dpg_bucket_batch {
   dpg_plan* plan;
   int C;
@@ -355,12 +364,21 @@ typedef struct dpg_bucket_batch {
 
 int dpg_assemble_multi(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags);
 
+/* Autotuner of the multi-bucket launch (no counterpart in the reference): times the
+ * work queue of the given single-CTA buckets with claim sizes 1, 2, 4 and 8 cells
+ * and returns the fastest in *chosen (pass it back as DPG_FLAG_CLAIM(*chosen); 1
+ * when there are only large buckets).  The per-bucket shapes come from
+ * dpg_plan_autotune on each plan beforehand. */
+int dpg_multi_autotune(int n_buckets, const dpg_bucket_batch* buckets, void* stream, int flags, int* chosen);
+
 /* The same multi-bucket launch recorded once in a CUDA graph and replayed:
  * for a fixed mesh re-assembled every step (new coefficients written into the
  * same buffers).  Capture uploads the bucket tables and allocates the
  * workspace (outside any stream capture of the caller); every launch then
- * reads the buffers named at capture time.  Launches of one graph must not
- * overlap on the GPU (they share the workspace). */
+ * reads the buffers named at capture time.  The graph holds the large buckets'
+ * launches in decreasing order of cost, then the work queue of the single-CTA
+ * buckets (whose counters reset themselves at the end of each launch).  Launches
+ * of one graph must not overlap on the GPU (they share the workspace). */
 typedef struct dpg_graph dpg_graph;
 int dpg_graph_capture(int n_buckets, const dpg_bucket_batch* buckets, int flags, dpg_graph** out);
 int dpg_graph_launch(dpg_graph* graph, void* stream);

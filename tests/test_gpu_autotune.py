@@ -1,9 +1,9 @@
 """dpg_plan_autotune: the per-bucket choice of the Gram staging chunk (8 or 4 quadrature points,
-which sets the shared-memory layout and the kernel instance) timed on the caller's cells.  After
+which sets the shared-memory layout and the kernel instance) or, for large buckets, of the
+formation k-chunk (32 or 16 points), timed on the caller's cells.  After
 tuning, the plan's results still match the oracle at the parity bar (relative Frobenius error
 <= 1e-12 per cell, or, where the Gram conditioning puts two FP64 codes further apart, an error
-against the extended-precision truth at most three times the FP64 oracle's own); large-bucket plans
-have a single configuration and report 0."""
+against the extended-precision truth at most three times the FP64 oracle's own)."""
 import numpy as np
 import pytest
 
@@ -39,8 +39,18 @@ def test_autotuned_plan_matches_oracle(make, oracle_mod):
     check_against_truth(oracle_mod, bucket, nodes, par, co, o, ref)
 
 
-def test_autotune_large_bucket_has_one_configuration():
-    form, bucket, nodes, par = stokes2d(3, 2, 1, 1, 0.1)
+def test_autotune_large_bucket_picks_a_formation_chunk(oracle_mod):
+    """Large-bucket plans tune the formation k-chunk (32 or 16 points); afterwards the results
+    still match the oracle at the parity bar."""
+    form, bucket, nodes, par = stokes2d(3, 2, 2, 1, 0.1)
     plan = dlib.Plan(bucket)
-    co = coeffs_for(bucket, plan.info, nodes.shape[0])
-    assert plan.autotune(_dev(nodes), _dev(par), _dev(co)) == 0
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, plan.info, C)
+    dn, dp, dc = _dev(nodes), _dev(par), _dev(co)
+    assert plan.autotune(dn, dp, dc) in (16, 32)
+    out = plan.assemble(dn, dp, dc)
+    torch.cuda.synchronize()
+    o = {k: v.cpu().numpy() for k, v in out.items()}
+    assert (o["info"] == 0).all()
+    ref = oracle_mod.OraclePlan(bucket).assemble(nodes, par, co)
+    check_against_truth(oracle_mod, bucket, nodes, par, co, o, ref)
