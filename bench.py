@@ -62,7 +62,40 @@ def parse():
                         "uneven-cell workload on --c3-cells jittered cells, one warm-up launch and one timed "
                         "launch; prints one JSON line")
     p.add_argument("--c3-cells", type=int, default=148)
+    p.add_argument("--case", default=None, choices=["c2", "c4"],
+                   help="small case for profiler captures: the 2D Poisson k=4 (c2) or CDR k=3 (c4) bucket on "
+                        "--case-n x --case-n jittered quads, one warm-up launch and one timed launch; prints one "
+                        "JSON line")
+    p.add_argument("--case-n", type=int, default=64)
     return p.parse_args()
+
+
+def run_case(args):
+    """One launch of the c2 or c4 bucket on a small jittered quad mesh (small case for ncu)."""
+    import torch
+    from camellia2_b200 import abi, formulation as fm, lib, mesh
+    n = args.case_n
+    nodes, par = mesh.quad_grid(n, n, 0.2 if args.case == "c2" else 0.1, seed=1)
+    if args.case == "c2":
+        plan = lib.Plan(fm.PoissonFormulation(2).bucket(abi.TOPO_QUAD, 4, 2))
+        co = mesh.uniform_coeff(nodes.shape[0], 1, plan.info["n_points_total"], seed=1)
+    else:
+        plan = lib.Plan(fm.ConvectionDiffusionReactionFormulation(2).bucket(abi.TOPO_QUAD, 3, 2))
+        co = mesh.cdr_coeff(nodes.shape[0], plan.info, seed=1)
+    C = nodes.shape[0]
+    dev = lambda x: torch.as_tensor(np.ascontiguousarray(x)).cuda()  # noqa: E731
+    dn, dp, dc = dev(nodes), dev(par), dev(co)
+    out = plan.alloc_outputs(C)
+    plan.assemble(dn, dp, dc, out=out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.assemble(dn, dp, dc, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    print(json.dumps({"case": args.case, "N": plan.info["N"], "M": plan.info["M"], "cells": C, "ms": ms,
+                      "cells_per_s": C / ms * 1e3, "info_nonzero_cells": int((out["info"] != 0).sum().item())}))
 
 
 def run_c3_bucket(args):
@@ -462,6 +495,9 @@ def main():
         return
     if args.c3_bucket:
         run_c3_bucket(args)
+        return
+    if args.case:
+        run_case(args)
         return
     import torch
     import torch.distributed as dist
