@@ -282,61 +282,78 @@ struct Ctx {
   double* const invd_s = sm + (P).sm_invd;                                             \
   (void)flag_s; (void)mbar_s; (void)tri_s; (void)nodes_s; (void)coef_s; (void)invd_s;
 
-// Factor the diagonal tile k in place (one warp; lanes 0..7 hold rows), record
-// 1 / L_jj in invd[8k + j] and, when linv != nullptr, the inverse tile L_kk^-1
-// (AK layout) in linv[64 k].  First failing pivot (1-based) -> *flag (sign sgn).
+// Factor the diagonal tile k in place (one warp).  Every lane loads the lower triangle and
+// runs the whole factorisation in its own registers, so the pivot chain is eight reciprocal
+// square roots, each followed by one multiply and one FMA, with no shuffle on it; then lane
+// c < 8 forms column c of the inverse tile L_kk^-1 from the same registers.  Records
+// 1 / L_jj in invd[8k + j] and the inverse tile (AK layout) in linv[64 k].  First failing
+// pivot (1-based) -> *flag (sign sgn).
 __device__ __forceinline__ void factor_diag(double* __restrict__ T, int k, int* flag, int sgn, double* invd,
                                             double* linv) {
   const int lane = threadIdx.x & 31;
   double* Tkk = T + (k * (k + 1) / 2 + k) * 64;
-  double row[8];
-  const int r = lane & 7;
+  double a[36];  // a[r (r + 1) / 2 + c], c <= r
 #pragma unroll
-  for (int c = 0; c < 8; c++) row[c] = Tkk[ak(r, c)];
+  for (int r = 0; r < 8; r++)
+#pragma unroll
+    for (int c = 0; c <= r; c++) a[r * (r + 1) / 2 + c] = Tkk[ak(r, c)];
+  double iv[8];
   bool failed = false;
   int fail_j = 0;
 #pragma unroll
   for (int j = 0; j < 8; j++) {
-    double piv = __shfl_sync(0xffffffffu, row[j], j);
+    const double piv = a[j * (j + 1) / 2 + j];
     if (!(piv > 0.0) && !failed) { failed = true; fail_j = j; }
-    double inv = rsqrt(piv);
-    if (r == j) { row[j] = piv * inv; if (lane < 8) invd[k * 8 + j] = inv; }
-    else if (r > j) row[j] *= inv;
+    const double inv = rsqrt(piv);
+    iv[j] = inv;
+    a[j * (j + 1) / 2 + j] = piv * inv;
 #pragma unroll
-    for (int c = j + 1; c < 8; c++) {
-      double lcj = __shfl_sync(0xffffffffu, row[j], c);
-      if (r >= c) row[c] -= row[j] * lcj;
-    }
+    for (int r = j + 1; r < 8; r++) a[r * (r + 1) / 2 + j] *= inv;
+#pragma unroll
+    for (int c = j + 1; c < 8; c++)
+#pragma unroll
+      for (int r = c; r < 8; r++) a[r * (r + 1) / 2 + c] -= a[r * (r + 1) / 2 + j] * a[c * (c + 1) / 2 + j];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    // row r, columns 4q .. 4q+3 are contiguous in the AK layout
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+      for (int q = 0; q < 2; q++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int c0 = 4 * q + 2 * h;
+          const double v0 = (c0 <= r) ? a[r * (r + 1) / 2 + c0] : 0.0;
+          const double v1 = (c0 + 1 <= r) ? a[r * (r + 1) / 2 + c0 + 1] : 0.0;
+          *reinterpret_cast<double2*>(Tkk + (q * 8 + r) * 4 + 2 * h) = make_double2(v0, v1);
+        }
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) *reinterpret_cast<double2*>(invd + k * 8 + j) = make_double2(iv[j], iv[j + 1]);
+    if (failed && *flag == 0) *flag = sgn * (k * 8 + fail_j + 1);
+  }
+  // column c of L_kk^-1 by forward substitution (lane c)
+  const int c = lane & 7;
+  double x[8];
+#pragma unroll
+  for (int rr = 0; rr < 8; rr++) {
+    double v = (rr == c) ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < rr; m++) v -= a[rr * (rr + 1) / 2 + m] * x[m];
+    x[rr] = (rr < c) ? 0.0 : v * iv[rr];
   }
   if (lane < 8) {
 #pragma unroll
-    for (int c = 0; c < 8; c++) Tkk[ak(r, c)] = (c <= r) ? row[c] : 0.0;
+    for (int rr = 0; rr < 8; rr++) linv[k * 64 + ak(rr, c)] = x[rr];
   }
-  if (lane == 0 && failed && *flag == 0) *flag = sgn * (k * 8 + fail_j + 1);
-  if (linv) {
-    __syncwarp();
-    // column c of L_kk^-1 by forward substitution (lane c)
-    if (lane < 8) {
-      const int c = lane;
-      double x[8];
-#pragma unroll
-      for (int rr = 0; rr < 8; rr++) {
-        double v = (rr == c) ? 1.0 : 0.0;
-#pragma unroll
-        for (int m = 0; m < rr; m++) v -= Tkk[ak(rr, m)] * x[m];
-        x[rr] = (rr < c) ? 0.0 : v * invd[k * 8 + rr];
-      }
-#pragma unroll
-      for (int rr = 0; rr < 8; rr++) linv[k * 64 + ak(rr, c)] = x[rr];
-    }
-    __syncwarp();
-  }
+  __syncwarp();
 }
 
 // Blocked right-looking Cholesky of the leading nsteps tiles of a tile-lower
 // matrix with nb tiles in shared memory (AK tiles).  Look-ahead: while the warps
 // of sub-partitions 1..3 apply the trailing update of step k, warp 0 updates diagonal
-// tile k+1 first and factors it, so each step costs two barriers.  The panel multiplies by
+// tile k+1 first and factors it, so each step costs two barriers (warp 0 only arrives
+// at the first).  The panel multiplies by
 // the inverse diagonal tile (two DMMAs per tile).  linv (NBT x 64) receives the
 // inverses of the factored diagonal tiles; invd the inverse pivots.
 __device__ __noinline__ void tile_cholesky(int T_off, int nb, int nsteps, int flag_idx, int sgn, int tri_off,
@@ -363,7 +380,14 @@ __device__ __noinline__ void tile_cholesky(int T_off, int nb, int nsteps, int fl
       __syncwarp();
       *reinterpret_cast<double2*>(Tik + ak_cfrag(g, t)) = c;
     }
-    __syncthreads();
+    // warp 0 needs only its own panel tile (k+1, k) for what follows, so it signals the
+    // barrier without waiting at it; the other warps wait for every panel tile
+    if (warp == 0) {
+      asm volatile("bar.arrive 1, %0;" ::"n"(NT) : "memory");
+      __syncwarp();
+    } else {
+      asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+    }
     // trailing update: A_ij -= L_ik L_jk^T for k < j <= i < nb; warp 0 does (k+1, k+1) and factors it
     const int m = nb - 1 - k;
     const int ntr = m * (m + 1) / 2;
@@ -383,16 +407,28 @@ __device__ __noinline__ void tile_cholesky(int T_off, int nb, int nsteps, int fl
       // the update runs on the other three sub-partitions' warps: warps 4, 8, 12 stay
       // idle so that warp 0's serial diagonal factorisation has its sub-partition (issue
       // slots) to itself; it is the critical path of every step
+      // each warp takes a contiguous range of the row-major tile list, so consecutive
+      // tiles share row i and L_ik stays in registers
       const int hidx = warp - (warp >> 2) - 1;
-      for (int u = 1 + hidx; u < ntr; u += DPG_NWARPS - DPG_NWARPS / 4) {
-        int ij = tri[u];
-        int i = k + 1 + (ij & 255), j = k + 1 + (ij >> 8);
+      const int nwt = DPG_NWARPS - DPG_NWARPS / 4;
+      const int tb = (ntr - 1) / nwt, te = (ntr - 1) % nwt;
+      const int u0 = 1 + hidx * tb + min(hidx, te), u1 = u0 + tb + (hidx < te ? 1 : 0);
+      int lastI = -1;
+      double a0 = 0.0, a1 = 0.0;
+      for (int u = u0; u < u1; u++) {
+        const int ij = tri[u];
+        const int i = k + 1 + (ij & 255), j = k + 1 + (ij >> 8);
         double* Tij = T + (i * (i + 1) / 2 + j) * 64;
-        const double* Lik = T + (i * (i + 1) / 2 + k) * 64;
+        if (i != lastI) {
+          const double* Lik = T + (i * (i + 1) / 2 + k) * 64;
+          a0 = -Lik[lane];
+          a1 = -Lik[32 + lane];
+          lastI = i;
+        }
         const double* Ljk = T + (j * (j + 1) / 2 + k) * 64;
         double2 c = *reinterpret_cast<const double2*>(Tij + ak_cfrag(g, t));
-        dmma(c, -Lik[lane], Ljk[lane]);
-        dmma(c, -Lik[32 + lane], Ljk[32 + lane]);
+        dmma(c, a0, Ljk[lane]);
+        dmma(c, a1, Ljk[32 + lane]);
         *reinterpret_cast<double2*>(Tij + ak_cfrag(g, t)) = c;
       }
     }
