@@ -17,8 +17,9 @@
 //      test-operator value over the points of every segment and term touching the tile
 //      (TBF::stiffnessMatrix, BF.cpp:575-656; RHS.cpp:68-82).  The diagonal G tiles come
 //      first and give the scales S.
-//   3. Np steps of a blocked right-looking Cholesky: the diagonal block is factored in shared
-//      memory together with its inverse, the rows below it become L panels (the rows of
+//   3. Np steps of a blocked right-looking Cholesky: the 64 x 64 diagonal block is factored in
+//      shared memory as 8 x 8 tiles (the single-CTA kernel's tile Cholesky) and inverted by block
+//      forward substitution, the rows below it become L panels (the rows of
 //      W^T = (L^-1 E)^T, BF.cpp:987-988) and the trailing update subtracts L_I L_J^T
 //      (DSYRK, BF.cpp:993-1005).  The trailing block is then -E^T G^-1 E = -[[K, l], [l^T, .]].
 //   4. K, l are written out, the trailing block is negated, and nfp more steps over the field
@@ -356,8 +357,82 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
   }
 }
 
+// The diagonal block Z[k0 .. k0+w) (w <= 64, padded to 64 with a unit diagonal): factored as
+// 8 x 8 tiles in AK layout (in D) by the single-CTA kernel's blocked Cholesky (tile_cholesky:
+// look-ahead, diagonal tiles factored in registers), then X = L_kk^-1 by block forward
+// substitution, one warp per 8-column block (X_cc = L_cc^-1, X_ic = -L_ii^-1 sum_k L_ik X_kc),
+// into Xi (row-major, zero above the diagonal).  The first column whose pivot is not positive
+// goes to *fail (atomicMin).
+__device__ __forceinline__ void big_diag_block(const double* Z, int ld, int k0, int w, const BigSm& S, int* fail) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  constexpr int NBD = ZT / 8;                 // 8 tiles
+  constexpr int NTD = NBD * (NBD + 1) / 2;    // 36 lower tiles
+  double* const T = S.D;
+  double* const linv = S.LI;                  // [8][64] inverse diagonal tiles
+  double* const invd = S.LI + NBD * 64;       // [64]
+  int* const tri = reinterpret_cast<int*>(S.LI + NBD * 64 + ZT);
+  int* const flag = tri + 64;
+  __syncthreads();
+  for (int e = tid; e < NTD * 64; e += NT) {
+    const int tau = e >> 6, idx = e & 63;
+    int I = 0;
+    while ((I + 1) * (I + 2) / 2 <= tau) I++;
+    const int J = tau - I * (I + 1) / 2;
+    const int r = 8 * I + ((idx >> 2) & 7), c = 8 * J + (idx >> 5) * 4 + (idx & 3);
+    double v = (r == c) ? 1.0 : 0.0;
+    if (r < w && c <= r) v = Z[(size_t)(k0 + r) * ld + k0 + c];
+    T[e] = v;
+    if (idx == 0) tri[tau] = I | (J << 8);
+  }
+  if (tid == 0) *flag = 0;
+  __syncthreads();
+  tile_cholesky((int)(T - dpg_smem), NBD, NBD, (int)(flag - reinterpret_cast<int*>(dpg_smem)), 1,
+                (int)(reinterpret_cast<double*>(tri) - dpg_smem), (int)(invd - dpg_smem), (int)(linv - dpg_smem));
+  if (tid == 0 && *flag > 0) atomicMin(fail, k0 + *flag - 1);
+  if (warp < NBD) {
+    const int cb = warp;
+    double2 acc[NBD];
+#pragma unroll
+    for (int i = 0; i < NBD; i++)
+      acc[i] = (i == cb) ? make_double2(g == 2 * t ? 1.0 : 0.0, g == 2 * t + 1 ? 1.0 : 0.0) : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < NBD; k++) {
+      if (k >= cb) {
+        double y0, y1;
+        cfrag_to_bfrag(acc[k], lane, y0, y1);
+        const double* Li = linv + k * 64;
+        double2 x = make_double2(0.0, 0.0);
+        dmma(x, Li[lane], y0);
+        dmma(x, Li[32 + lane], y1);
+        acc[k] = x;
+        double x0, x1;
+        cfrag_to_bfrag(x, lane, x0, x1);
+        x0 = -x0;
+        x1 = -x1;
+#pragma unroll
+        for (int i = k + 1; i < NBD; i += 2) {
+          const double* Lik = T + (i * (i + 1) / 2 + k) * 64;
+          if (i + 1 < NBD) {
+            const double* Li1k = T + ((i + 1) * (i + 2) / 2 + k) * 64;
+            dmma16x8(acc[i], acc[i + 1], Lik[lane], Li1k[lane], Lik[32 + lane], Li1k[32 + lane], x0, x1);
+          } else {
+            dmma(acc[i], Lik[lane], x0);
+            dmma(acc[i], Lik[32 + lane], x1);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NBD; i++)
+      *reinterpret_cast<double2*>(S.Xi + (8 * i + g) * ZL + 8 * cb + 2 * t) = acc[i];
+  }
+  __syncthreads();
+}
+
 // Steps kb .. ke-1 of a right-looking Cholesky of the lower triangle of Z (order Zn).  The
-// first column whose pivot is not positive goes to *fail (atomicMin); its pivot is taken as 1.
+// first column whose pivot is not positive goes to *fail (atomicMin); the cell's outputs are
+// then undefined (info reports the column).
 __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, const BigSm& S, int* fail) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -366,42 +441,7 @@ __device__ void big_cholesky(const DpgPlanDev& P, double* Z, int kb, int ke, con
   for (int k0 = kb; k0 < ke; k0 += ZT) {
     const int w = min(ZT, ke - k0);
     const int wk = (w + 15) & ~15;
-    __syncthreads();
-    for (int e = tid; e < ZT * ZT; e += NT) {
-      const int r = e >> 6, c = e & (ZT - 1);
-      S.D[r * ZL + c] = (r < w && c <= r) ? Z[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
-      S.Xi[r * ZL + c] = (r == c) ? 1.0 : 0.0;
-    }
-    __syncthreads();
-    // L_kk and L_kk^-1 together: column j of L (also copied to a contiguous vector, LI's first
-    // row, free until the panels), row j of the inverse, then the updates: 8 rows x 64 columns
-    // per pass of the block
-    double* const colj = S.LI;
-    for (int j = 0; j < w; j++) {
-      double piv = S.D[j * ZL + j];
-      if (!(piv > 0.0)) {
-        if (tid == 0) atomicMin(fail, k0 + j);
-        piv = 1.0;
-      }
-      const double rinv = 1.0 / sqrt(piv);
-      if (tid < ZT) {
-        if (tid > j && tid < w) {
-          const double v = S.D[tid * ZL + j] * rinv;
-          S.D[tid * ZL + j] = v;
-          colj[tid] = v;
-        }
-        if (tid <= j) S.Xi[j * ZL + tid] *= rinv;
-      }
-      __syncthreads();
-      const int c = tid & (ZT - 1);
-      if (c < w)
-        for (int r = j + 1 + (tid >> 6); r < w; r += NT / ZT) {
-          const double lrj = colj[r];
-          if (c <= j) S.Xi[r * ZL + c] -= lrj * S.Xi[j * ZL + c];
-          else if (c <= r) S.D[r * ZL + c] -= lrj * colj[c];
-        }
-      __syncthreads();
-    }
+    big_diag_block(Z, ld, k0, w, S, fail);
     // rows below the block: panel L_I = Z_I,k L_kk^-T (stored back), then Z_IJ -= L_I L_J^T
     const int rbeg = k0 + w;
     const int nrb = (Zn - rbeg + ZT - 1) / ZT;
