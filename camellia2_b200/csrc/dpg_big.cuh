@@ -241,25 +241,35 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
   // kind 1: each thread's k index only grows (chunk by chunk, and with u inside a chunk), so the
   // entry holding it is found by a forward cursor per side instead of a scan from the start
   int ecur[2] = {0, 0};
+  // A thread forms KPT consecutive k of each side.  G tiles number k point-major (k = q nrel +
+  // row), so a thread's run mostly stays on one point and reads its column's four reference slot
+  // values once for all the IP rows.
+  constexpr int KPT = ZK / (NT / ZT);
   auto operands = [&](int k0, int buf) {
     double* const fa = S.fa + buf * 2 * ZK * ZL;
     double vals[NU];
+    int lastq = -1;
+    double fv[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int u = 0; u < NU; u++) {
-      const int e = tid + u * NT;
-      const int side = e / (ZK * ZT), kl = (e >> 6) & (ZK - 1);
+      const int side = u / KPT, kl = (tid >> 6) * KPT + (u % KPT);
+      if (u % KPT == 0) lastq = -1;
       const int kk = k0 + kl;
       double val = 0.0;
       if (kk < nk) {
         if (kind == 0) {
           const int rec = crec[side];
           if (rec >= 0) {
-            const int ri = kk / P.QG, q = kk - ri * P.QG, r = rel[ri];
+            const int q = kk / nrel, r = rel[kk - q * nrel];
             const int a = rec >> 16;
-            const int ld = P.test[a].ldA;
+            if (q != lastq) {
+              const int ld = P.test[a].ldA;
+              const double* f = P.frefG + (size_t)q * P.featstride + P.test[a].foff + (rec & 0xffff);
+              fv[0] = __ldg(f); fv[1] = __ldg(f + ld); fv[2] = __ldg(f + 2 * ld); fv[3] = __ldg(f + 3 * ld);
+              lastq = q;
+            }
             const double* b = bh + ((size_t)(q * P.niprows + r) * P.ntest + a) * 4;
-            const double* f = P.frefG + (size_t)q * P.featstride + P.test[a].foff + (rec & 0xffff);
-            val = b[0] * __ldg(f) + b[1] * __ldg(f + ld) + b[2] * __ldg(f + 2 * ld) + b[3] * __ldg(f + 3 * ld);
+            val = b[0] * fv[0] + b[1] * fv[1] + b[2] * fv[2] + b[3] * fv[3];
             if (side == 0) val *= wq[q];
           }
         } else {
@@ -289,8 +299,7 @@ __device__ void big_form_tile(const DpgPlanDev& P, const DpgLaunch& L, int kind,
     }
 #pragma unroll
     for (int u = 0; u < NU; u++) {
-      const int e = tid + u * NT;
-      const int side = e / (ZK * ZT), kl = (e >> 6) & (ZK - 1);
+      const int side = u / KPT, kl = (tid >> 6) * KPT + (u % KPT);
       fa[side * ZK * ZL + kl * ZL + cc] = vals[u];
     }
   };
