@@ -167,3 +167,30 @@ def test_big_bucket_energy_error_matches_oracle(name, oracle_mod):
         r = F[c] - B[c].T @ x[c]
         ref = np.sqrt(r @ np.linalg.solve(G[c], r))
         assert abs(e[c] - ref) <= 1e-10 * ref, (c, e[c], ref)
+
+
+@pytest.mark.parametrize("make", [lambda: stokes2d(3, 2, 2, 2, 0.1), lambda: stokes2d(6, 2, 2, 1, 0.1),
+                                  lambda: poisson2d(2, 2, 2, 2, 0.1)],
+                         ids=["large_k3", "large_k6", "single_cta"])
+def test_failed_factorisation_reports_the_oracle_info(make, oracle_mod):
+    """A cell mirrored in x has det J < 0: its Gram matrix is negative definite, the factored
+    Cholesky fails at the first pivot, and info holds the same 1-based column as the oracle's
+    (DPOTRF INFO).  The other cells' outputs are bitwise those of a run without the bad cell."""
+    form, bucket, nodes, par = make()
+    P = oracle_mod.OraclePlan(bucket)
+    C = nodes.shape[0]
+    co = coeffs_for(bucket, P.info, C)
+    bad = nodes.copy()
+    bad[1, :, 0] = -bad[1, :, 0]
+    ref = P.assemble(bad, par, co)
+    plan = dlib.Plan(bucket)
+    dco = None if co is None else _dev(co)
+    good = {k: v.cpu().numpy() for k, v in plan.assemble(_dev(nodes), _dev(par), dco).items()}
+    out = {k: v.cpu().numpy() for k, v in plan.assemble(_dev(bad), _dev(par), dco).items()}
+    torch.cuda.synchronize()
+    assert ref["info"][1] != 0
+    assert out["info"][1] == ref["info"][1]
+    keep = np.arange(C) != 1
+    assert (out["info"][keep] == 0).all() and (ref["info"][keep] == 0).all()
+    for k in ("K", "l", "S", "s"):
+        assert np.array_equal(out[k][keep], good[k][keep]), k
