@@ -614,6 +614,17 @@ __device__ __forceinline__ void big_cell_body(const DpgPlanDev& P, const DpgLaun
         // a failed factorisation of the test block leaves no energy to report
         L.energy[cell] = S.ints[0] == BIG_NOFAIL ? sqrt(e2) : __longlong_as_double(0x7ff8000000000000ll);
       }
+    } else if (L.B) {
+      // DLS local matrices (dpg_assemble_dls): the rows below the test block hold
+      // W^T = (L^-1 E)^T, so W = L^-1 B^T and y = L^-1 F are read out in user numbering
+      const int N = P.N;
+      double* Wc = L.B + (size_t)cell * M * N;
+      for (size_t e = tid; e < (size_t)M * N; e += NT) {
+        const int ut = (int)(e / N), us = (int)(e - (size_t)ut * N);
+        Wc[e] = Z[(size_t)(Np + __ldg(P.u2d_trial + ut)) * ld + __ldg(P.u2d_test + us)];
+      }
+      if (L.F)
+        for (int us = tid; us < N; us += NT) L.F[(size_t)cell * N + us] = Z[(size_t)(Np + P.fcol) * ld + __ldg(P.u2d_test + us)];
     } else {
     // trailing block = -[K_ext]: K, l out, then negate (padded field columns get a unit pivot)
     const double* T = Z + (size_t)Np * ld + Np;

@@ -1768,10 +1768,7 @@ int dpg_launch_adjoint(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_
 
 int dpg_launch_energy(const DpgPlanDev* plan, const DpgLaunch* Lin, cudaStream_t stream) {
   if (Lin->C <= 0) return DPG_OK;
-  if (plan->big) {
-    if (!Lin->xsol) return dpg::fail(DPG_ERR_UNSUPPORTED, "large-bucket plans have no DLS output");
-    return launch_big(plan, Lin, stream);
-  }
+  if (plan->big) return launch_big(plan, Lin, stream);  // energy error or DLS output
   KernelFn k = Lin->xsol ? pick_energy_kernel(plan) : pick_dls_kernel(plan);
   if (!k) return dpg::fail(DPG_ERR_UNSUPPORTED, "no kernel instance for this bucket size");
   int dev = 0, optin = 0;

@@ -197,8 +197,8 @@ typedef struct dpg_plan dpg_plan;
  * trial dofs after padding get a plan for the large-bucket kernel (matrices in
  * a per-SM global workspace taken from the stream-ordered pool at each call);
  * such plans support dpg_assemble, dpg_assemble_host, dpg_assemble_parts,
- * dpg_energy_error, dpg_assemble_multi and the graph calls, and the other
- * entry points return DPG_ERR_UNSUPPORTED. */
+ * dpg_energy_error, dpg_assemble_dls, dpg_assemble_multi and the graph calls,
+ * and the other entry points return DPG_ERR_UNSUPPORTED. */
 int dpg_plan_create(const dpg_bucket_desc* desc, dpg_plan** plan);
 int dpg_plan_destroy(dpg_plan* plan);
 int dpg_plan_query(const dpg_plan* plan, dpg_plan_info* info);
