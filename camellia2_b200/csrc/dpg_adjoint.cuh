@@ -167,12 +167,22 @@ __device__ __forceinline__ void adj_feature_gemm(const DpgPlanDev& P, const DpgL
       const double* f0 = fs + q0 * fsl + V.foff + k * V.ldA + t;
       const double* f1 = fs + q1 * fsl + V.foff + k * V.ldA + t;
       const bool ok0 = q0 < nq, ok1 = q1 < nq;
-      for (int i = 0; i < V.ntiles * 8; i += 4) {
-        const int row = V.ntile0 * 8 + i + t;
-        const double b = src[cfrag_index(P.NBT, row, J * 8 + g)];
-        dmma(acc0, ok0 ? f0[i] : 0.0, b);
-        dmma(acc1, ok1 ? f1[i] : 0.0, b);
+      // 16 test rows per m16n8k16: A rows g = (point q0, slot k), rows g + 8 = (point q1, slot k)
+      // (the vars' rows are padded to multiples of 16); the same accumulation order as four
+      // m8n8k4 steps per point pair
+      double c4[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int i = 0; i < V.ntiles * 8; i += 16) {
+        double av[8], bv[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          av[2 * j] = ok0 ? f0[i + 4 * j] : 0.0;
+          av[2 * j + 1] = ok1 ? f1[i + 4 * j] : 0.0;
+          bv[j] = src[cfrag_index(P.NBT, V.ntile0 * 8 + i + 4 * j + t, J * 8 + g)];
+        }
+        dmma16(c4, av, bv);
       }
+      acc0 = make_double2(c4[0], c4[1]);
+      acc1 = make_double2(c4[2], c4[3]);
       // C-fragment rows g -> (point 2R + g / 4, slot g % 4), columns 2t, 2t + 1
       if (ok0) *reinterpret_cast<double2*>(out + ((q0 * P.ntest + a) * 4 + k) * P.a_ldx + ct * 8 + 2 * t) = acc0;
       if (ok1) *reinterpret_cast<double2*>(out + ((q1 * P.ntest + a) * 4 + k) * P.a_ldx + ct * 8 + 2 * t) = acc1;
